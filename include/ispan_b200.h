@@ -1,0 +1,124 @@
+/*
+ * ispan_b200.h -- C ABI of the B200 (sm_100a) strongly-connected-component
+ * engine.  Drop-in for iSpan's detection call.
+ *
+ * Reference interface replaced (paths inside the iSpan tree):
+ *   void scc_detection(const graph *g, int alpha, int beta, int gamma,
+ *                      double theta, index_t thread_count, double *avg_time)
+ *       src/scc_common.h:15-23, defined at src/scc_core.cpp:27-1094
+ *   void get_scc_result(index_t *scc_id, index_t vert_count)
+ *       src/scc_common.h:25-28 (link-time hook, src/load_print.cpp:24-60)
+ *   class graph {fw_beg_pos, fw_csr, bw_beg_pos, bw_csr, vert_count,
+ *                edge_count}   src/graph.h:9-31, loaded by src/graph.cpp:2-92
+ *
+ * Plain pointers and sizes only.  Every call returns ISPAN_OK (0) or a
+ * negative ISPAN_ERR_* code; nothing exits the process (the reference's
+ * loader exits or asserts, src/graph.cpp:18-26).
+ */
+#ifndef ISPAN_B200_H
+#define ISPAN_B200_H
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ISPAN_OK 0
+#define ISPAN_ERR_ARG (-1)       /* bad argument or malformed CSR */
+#define ISPAN_ERR_NOMEM (-2)     /* device allocation or HBM budget exceeded */
+#define ISPAN_ERR_CUDA (-3)      /* a CUDA runtime call failed */
+#define ISPAN_ERR_TIMEOUT (-4)   /* a bounded device-side wait ran out */
+#define ISPAN_ERR_INTERNAL (-5)  /* a device-side capacity check failed */
+#define ISPAN_ERR_NODEV (-6)     /* no CUDA device / kernels not loadable */
+#define ISPAN_ERR_CAPACITY (-7)  /* graph larger than the context was sized for */
+
+/* One directed graph in the reference's CSR layout (src/graph.h:9-31):
+ * fw_beg/fw_adj = out-edges, bw_beg/bw_adj = in-edges (the transpose).
+ * Offsets are int32 (the reference's width) or int64 (offset_bytes = 8),
+ * vertex ids int32.  on_device = 1 when all four pointers are device memory
+ * of the context's GPU; 0 when they are host memory (pinned memory uploads
+ * fastest). */
+typedef struct {
+    int64_t V, E;
+    const void *fw_beg, *bw_beg;
+    const int32_t *fw_adj, *bw_adj;
+    int32_t offset_bytes;
+    int32_t on_device;
+} ispan_csr;
+
+/* Direction-switch parameters of the reference's reachability searches
+ * (src/fw_bw.h:576-624; CLI order of src/scc_main.cpp:16-25).  alpha: switch
+ * top-down -> bottom-up when frontier edges exceed unexplored edges / alpha;
+ * beta, gamma: switch bottom-up -> queue top-down when the frontier falls
+ * below |worklist| / beta or the level exceeds gamma.  theta is the
+ * reference's trim stop ratio; the peel here runs to a fixpoint, so theta is
+ * accepted and recorded only.  Zero fields take the reference defaults
+ * 30/200/10/0.1 (src/bash_one.sh:4). */
+typedef struct {
+    int32_t alpha, beta, gamma;
+    double theta;
+    uint32_t flags;
+} ispan_params;
+
+#define ISPAN_F_LABELS_ON_DEVICE 1u /* labels_out is device memory */
+#define ISPAN_F_NO_GRAPH 2u         /* launch stages directly, no CUDA graph */
+#define ISPAN_F_STAGE_TIMES 4u      /* record per-stage device times */
+#define ISPAN_F_NO_L2_WINDOW 8u     /* do not pin the status maps in L2 */
+
+/* Stage-time slots follow the reference's avg_time[15] meanings
+ * (src/scc_core.cpp:24-25, :1037-1053): 0 trim, 1 elephant SCC, 2 mice SCC,
+ * 3 total, 4 trim size_1, 5 trim size_2, 6 pivot selection, 7 FW, 8 BW,
+ * 9 WCC, 10 mice FW-BW, 13 trim size_3.  Milliseconds of device time. */
+typedef struct {
+    double stage_ms[16];
+    int64_t scc_count;        /* number of SCCs (no phantom vertex, unlike Q1) */
+    int64_t giant_size;       /* vertices of the pivot SCC(s) */
+    int64_t n_trim1, n_trim2, n_trim3; /* vertices labelled by each trim */
+    int64_t n_mice_vertices, n_mice_scc, n_wcc;
+    int64_t fw_size, fw_levels, bw_levels, residual, color_rounds, local_wcc, trim_rounds;
+    /* sparse size histogram: pairs (hist_size[i], hist_count[i]) sorted by
+     * size; the caller supplies the arrays (hist_cap entries) or NULLs */
+    int64_t *hist_size, *hist_count;
+    int64_t hist_cap, hist_n;
+} ispan_stats;
+
+typedef struct ispan_ctx ispan_ctx;
+
+/* A context owns device scratch for graphs up to max_V vertices / max_E
+ * edges (per run) on one device, plus a CUDA stream (or the caller's stream
+ * set with ispan_ctx_set_stream).  Contexts are independent; one context must
+ * not be used by two host threads at once. */
+int ispan_ctx_create(int device, int64_t max_V, int64_t max_E, ispan_ctx **out);
+int ispan_ctx_destroy(ispan_ctx *ctx);
+int ispan_ctx_set_stream(ispan_ctx *ctx, void *cuda_stream);
+/* device bytes a context of this size holds (without uploaded graphs) */
+int64_t ispan_ctx_bytes(int64_t max_V, int64_t max_E);
+
+/* Detect the SCCs of g.  labels_out[V] receives, for every vertex, the
+ * minimum vertex id of its SCC (host memory unless ISPAN_F_LABELS_ON_DEVICE).
+ * Replaces scc_detection (src/scc_core.cpp:27); st may be NULL. */
+int ispan_scc_run(ispan_ctx *ctx, const ispan_csr *g, const ispan_params *p,
+                  int32_t *labels_out, ispan_stats *st);
+
+/* Batched form: g is a disjoint union of nseg graphs whose vertex ranges are
+ * [vbase[i], vbase[i+1]) (vbase host array of nseg+1 entries, vbase[0] = 0,
+ * vbase[nseg] = V; edges never cross ranges).  Every graph gets its own pivot
+ * and giant search; labels are global vertex ids (subtract vbase[i] for a
+ * graph-local id).  One set of stage launches covers all graphs. */
+int ispan_scc_run_batch(ispan_ctx *ctx, const ispan_csr *g, int32_t nseg, const int64_t *vbase,
+                        const ispan_params *p, int32_t *labels_out, ispan_stats *st);
+
+/* Reference-convention per-vertex codes from canonical labels and the class
+ * of each vertex, as get_scc_result (src/load_print.cpp:24-60) expects:
+ * 1 giant, -1 trimmed size-1, -2 size-2, -3 size-3, otherwise label + 2;
+ * codes_out has V+1 entries, the last (the reference's phantom slot) 0.
+ * Valid after the most recent run on ctx; host memory. */
+int ispan_ref_codes(ispan_ctx *ctx, int32_t *codes_out);
+
+const char *ispan_strerror(int code);
+/* library version string */
+const char *ispan_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

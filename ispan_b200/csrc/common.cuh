@@ -1,0 +1,280 @@
+// common.cuh -- device-side building blocks shared by every stage kernel of
+// the B200 SCC pipeline: the run descriptor, 1-bit-per-vertex status maps,
+// warp-aggregated queue appends, block reductions and a bounded grid barrier
+// for the persistent (cooperatively launched) stage kernels.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/ispan_b200.h"
+
+namespace ispan {
+
+constexpr int kBlock = 512;           // threads per CTA for persistent stages
+constexpr int kWarps = kBlock / 32;
+constexpr int kChunk = 4096;          // edges per top-down work chunk (8 per thread)
+constexpr unsigned kFull = 0xffffffffu;
+constexpr int kCountBits = 31;        // packed queue counter: count | edges << 31
+constexpr uint64_t kCountMask = (1ull << kCountBits) - 1;
+
+// ---------------------------------------------------------------------------
+// Run descriptor.  One CSR (or a disjoint union of graphs, `nseg` segments
+// with vertex bases vbase[0..nseg]) plus every scratch array of the context.
+// Vertex state lives in bitmaps of 32-bit words so the status of all vertices
+// of a 40 M-vertex graph (5 MB per map) stays resident in the 126 MB L2.
+template <typename OffT>
+struct Run {
+    int64_t V, E, W;              // vertices, edges, bitmap words
+    int32_t nseg;
+    const int64_t *vbase;         // [nseg+1] vertex base of each graph
+    const OffT *fw_beg, *bw_beg;  // [V+1]
+    const int32_t *fw_adj, *bw_adj;
+    int32_t *label;               // [V] output: canonical (min-id) SCC label
+
+    uint32_t *A;      // active: not yet assigned to an SCC
+    uint32_t *F;      // forward-reached (giant) / mark map in later stages
+    uint32_t *B;      // backward-reached (giant) / second mark map
+    uint32_t *D;      // dead: claimed by a trim in the current stage
+    uint32_t *P;      // snapshot of the visit map at the start of a bottom-up level
+
+    // frontier queues (double buffered): vertex, edge prefix, chunk -> slot
+    int32_t *qv[2];
+    int64_t *qe[2];
+    int32_t *qchunk[2];
+    unsigned long long *qpk;      // [3] packed counters (count | edges << 31)
+    unsigned long long *lvl;      // [3 * 4] per-level stats slots
+
+    // residual worklist (double buffered) and its counters
+    int32_t *wl[2];
+    unsigned long long *wlc;      // [4]
+
+    int32_t *cnt_out, *cnt_in;    // [V] active out/in degree counters (trim-1)
+    int32_t *parent;              // [V] WCC union-find / colour labels
+    int32_t *aux;                 // [V] grouping scratch (counts, offsets)
+    int32_t *aux2;                // [V]
+    int32_t *members;             // [V] vertices grouped by WCC
+
+    unsigned long long *pivot_key; // [nseg] (product << 32) | ~id
+    int32_t *gmin;                // [nseg] min id of each giant SCC
+    unsigned long long *gsize;    // [nseg] size of each giant SCC
+    uint8_t *cls;                 // [V] class of each vertex (for reference codes)
+    unsigned long long *counters; // [kNumCounters] statistics
+    int64_t *hist;                // [kHistCap] SCC size histogram (sizes < cap)
+    unsigned int *gsync;          // [2] grid barrier (count, generation)
+    int *err;                     // [4] error word, detail
+    int32_t alpha, beta, gamma;
+    uint32_t flags;
+};
+
+// statistics counters (indices into Run::counters)
+enum Counter {
+    C_ACTIVE0 = 0,   // active after trim-1-first
+    C_MU0,           // sum of out-degrees of the active vertices
+    C_FW_SIZE,       // |F|
+    C_FW_MU,         // sum of in-degrees over F (bottom-up budget of the BW search)
+    C_GIANT,         // |S| over all segments
+    C_TRIM1,         // vertices labelled by trim-1 (first pass + peels)
+    C_TRIM2,         // vertices in trim-2 pairs
+    C_TRIM3,         // vertices in trim-3 triples
+    C_MICE_V,        // vertices labelled by the mice stage
+    C_MICE_SCC,      // SCCs found by the mice stage
+    C_WCC,           // weakly connected components entering the mice stage
+    C_FW_LEVELS,
+    C_BW_LEVELS,
+    C_RESID,         // residual after the giant
+    C_COLOR_ROUNDS,  // colouring rounds of the large-WCC path
+    C_LOCAL_WCC,     // WCCs solved in shared memory
+    C_BIG,           // SCC sizes >= hist cap (listed separately)
+    C_TRIM_ROUNDS,
+    C_GIANTS,        // graphs whose pivot SCC is non-empty
+    C_SPILL,         // small WCCs whose edges overflowed shared memory
+    kNumCounters = 32
+};
+constexpr int kHistCap = 1 << 16;   // exact histogram for SCC sizes below this
+constexpr int kBigCap = 1 << 16;    // list of larger SCC sizes (hist[kHistCap..])
+
+// error codes mirror ispan_b200.h
+constexpr int kErrTimeout = ISPAN_ERR_TIMEOUT;
+constexpr int kErrOverflow = ISPAN_ERR_INTERNAL;
+
+// ---------------------------------------------------------------------------
+// small helpers
+__device__ __forceinline__ bool bit(const uint32_t *m, int64_t v) {
+    return (__ldg(m + (v >> 5)) >> (v & 31)) & 1u;
+}
+// coherent bit read (L2, not L1 or the read-only path): for maps that other
+// CTAs change while this kernel runs
+__device__ __forceinline__ bool bitv(const uint32_t *m, int64_t v) {
+    return (__ldcg(m + (v >> 5)) >> (v & 31)) & 1u;
+}
+__device__ __forceinline__ bool bitc(const uint32_t *m, int64_t v) {
+    return (m[v >> 5] >> (v & 31)) & 1u;
+}
+// set a bit; returns true if this call changed it from 0 to 1
+__device__ __forceinline__ bool set_bit(uint32_t *m, int64_t v) {
+    uint32_t b = 1u << (v & 31);
+    return !(atomicOr(m + (v >> 5), b) & b);
+}
+__device__ __forceinline__ void clear_bit(uint32_t *m, int64_t v) {
+    atomicAnd(m + (v >> 5), ~(1u << (v & 31)));
+}
+__device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
+__device__ __forceinline__ unsigned lanemask_lt() {
+    unsigned m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+__device__ __forceinline__ uint64_t globaltimer() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+template <typename OffT>
+__device__ __forceinline__ int64_t ld_off(const OffT *p, int64_t i) { return (int64_t)__ldg(p + i); }
+
+__device__ __forceinline__ int64_t warp_sum64(int64_t x) {
+#pragma unroll
+    for (int o = 16; o; o >>= 1) x += __shfl_xor_sync(kFull, x, o);
+    return x;
+}
+__device__ __forceinline__ int64_t warp_incl_scan64(int64_t x) {
+    int l = lane_id();
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int64_t y = __shfl_up_sync(kFull, x, o);
+        if (l >= o) x += y;
+    }
+    return x;
+}
+__device__ __forceinline__ int warp_min(int x) {
+#pragma unroll
+    for (int o = 16; o; o >>= 1) x = min(x, __shfl_xor_sync(kFull, x, o));
+    return x;
+}
+__device__ __forceinline__ unsigned long long warp_max_u64(unsigned long long x) {
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+        unsigned long long y = __shfl_xor_sync(kFull, x, o);
+        x = y > x ? y : x;
+    }
+    return x;
+}
+
+// Block-wide sum of one int64 per thread; result valid in every thread.
+// Needs kBlock threads and the caller's shared scratch of kWarps entries.
+__device__ __forceinline__ int64_t block_sum64(int64_t x, int64_t *sh) {
+    x = warp_sum64(x);
+    __syncthreads();
+    if (lane_id() == 0) sh[threadIdx.x >> 5] = x;
+    __syncthreads();
+    int64_t t = 0;
+#pragma unroll
+    for (int i = 0; i < kWarps; ++i) t += sh[i];
+    return t;
+}
+
+// ---------------------------------------------------------------------------
+// Bounded grid barrier for a cooperatively launched (co-resident) grid.
+// Thread 0 of every CTA arrives on a counter; the last one bumps the
+// generation.  Waiters poll the generation with %globaltimer as the bound: on
+// timeout the error word is set and every CTA leaves the barrier reporting
+// failure, so the stage kernel returns instead of hanging.
+constexpr uint64_t kBarrierTimeoutNs = 20ull * 1000 * 1000 * 1000;  // 20 s
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned *p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_u32(unsigned *p, unsigned v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ int ld_volatile_int(const int *p) { return *(volatile const int *)p; }
+
+__device__ __noinline__ bool grid_sync(unsigned *gs, int *err) {
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ok = ld_volatile_int(err) == 0;
+        unsigned gen = ld_acquire_u32(gs + 1);
+        __threadfence();
+        unsigned arrived = atomicAdd(gs, 1u);
+        if (arrived == gridDim.x - 1) {
+            atomicExch(gs, 0u);
+            __threadfence();
+            st_release_u32(gs + 1, gen + 1);
+        } else {
+            uint64_t t0 = globaltimer();
+            while (ld_acquire_u32(gs + 1) == gen) {
+                if (ld_volatile_int(err) != 0) { ok = 0; break; }
+                __nanosleep(64);
+                if (globaltimer() - t0 > kBarrierTimeoutNs) {
+                    atomicCAS(err, 0, kErrTimeout);
+                    ok = 0;
+                    break;
+                }
+            }
+        }
+        __threadfence();
+        if (ld_volatile_int(err) != 0) ok = 0;
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok;
+}
+
+// ---------------------------------------------------------------------------
+// Warp-aggregated append of (vertex, degree) into a frontier queue whose
+// packed counter reserves slots and edge ranges in one 64-bit atomic, so the
+// queue is an exclusive prefix over edges in slot order.  Each chunk boundary
+// c*kChunk that falls inside the appended vertex's edge range records the
+// slot, which lets a consumer map a chunk to its slots in O(1).
+// Must be called by all 32 lanes of a warp (pred selects the appenders).
+__device__ __forceinline__ void q_append(bool pred, int32_t v, int64_t deg, int32_t *qv, int64_t *qe,
+                                         int32_t *qchunk, unsigned long long *pk, int64_t cap_v) {
+    unsigned m = __ballot_sync(kFull, pred && deg > 0);
+    if (!m) return;
+    bool me = (m >> lane_id()) & 1u;
+    int64_t d = me ? deg : 0;
+    int64_t incl = warp_incl_scan64(d);
+    int64_t tot = __shfl_sync(kFull, incl, 31);
+    int leader = __ffs(m) - 1;
+    unsigned long long base = 0;
+    if (lane_id() == leader)
+        base = atomicAdd(pk, ((unsigned long long)tot << kCountBits) | (unsigned long long)__popc(m));
+    base = __shfl_sync(kFull, base, leader);
+    if (me) {
+        int64_t slot = (int64_t)(base & kCountMask) + __popc(m & lanemask_lt());
+        int64_t eb = (int64_t)(base >> kCountBits) + incl - d;
+        if (slot < cap_v) {
+            qv[slot] = v;
+            qe[slot] = eb;
+            int64_t c0 = (eb + kChunk - 1) / kChunk, c1 = (eb + d - 1) / kChunk;
+            for (int64_t c = c0; c <= c1; ++c) qchunk[c] = (int32_t)slot;
+        }
+    }
+}
+
+// Warp-aggregated append of a vertex id to a plain worklist.
+__device__ __forceinline__ void wl_append(bool pred, int32_t v, int32_t *wl, unsigned long long *cnt) {
+    unsigned m = __ballot_sync(kFull, pred);
+    if (!m) return;
+    int leader = __ffs(m) - 1;
+    unsigned long long base = 0;
+    if (lane_id() == leader) base = atomicAdd(cnt, (unsigned long long)__popc(m));
+    base = __shfl_sync(kFull, base, leader);
+    if (pred) wl[base + __popc(m & lanemask_lt())] = v;
+}
+
+// segment of a vertex in a disjoint union (binary search over vbase)
+__device__ __forceinline__ int seg_of(const int64_t *vbase, int nseg, int64_t v) {
+    if (nseg == 1) return 0;
+    int lo = 0, hi = nseg - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (__ldg(vbase + mid) <= v) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+}  // namespace ispan

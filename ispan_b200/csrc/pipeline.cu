@@ -1,0 +1,676 @@
+// pipeline.cu -- host side of the B200 SCC engine: contexts, device memory,
+// the stage launch sequence (captured once into a CUDA graph and replayed),
+// and the extern "C" boundary declared in include/ispan_b200.h.
+//
+// Stage sequence (reference src/scc_core.cpp:144-1070, same order):
+//   trim-1-first + pivot      k_trim1_first, k_seed
+//   elephant FW / BW          k_bfs<.,0>, k_bfs<.,1>   (persistent, cooperative)
+//   giant, residual           k_giant, k_residual
+//   trim-1 peel (fixpoint)    k_trim1                  (persistent, cooperative)
+//   trim-2, trim-3            k_trim2, k_trim3
+//   trim-1 peel again         k_trim1
+//   WCC                       k_wcc_init/hook/flatten/alloc/scatter
+//   mice: small WCCs          k_local_scc              (shared-memory Tarjan)
+//   mice: large WCCs          k_color                  (persistent, cooperative)
+//   canonical labels          k_finalize
+// Every kernel reads its work sizes from device memory, so the whole sequence
+// is enqueued without a host round trip and the host synchronises once.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "bfs.cuh"
+#include "stages.cuh"
+
+using namespace ispan;
+
+namespace {
+
+#define CK(x)                                                                        \
+    do {                                                                             \
+        cudaError_t e_ = (x);                                                        \
+        if (e_ != cudaSuccess) {                                                     \
+            fprintf(stderr, "ispan_b200: %s failed: %s (%s:%d)\n", #x, cudaGetErrorString(e_), \
+                    __FILE__, __LINE__);                                             \
+            return ISPAN_ERR_CUDA;                                                   \
+        }                                                                            \
+    } while (0)
+
+template <typename T>
+static int dalloc(T **p, size_t n, std::vector<void *> &owned) {
+    if (n == 0) n = 1;
+    void *q = nullptr;
+    if (cudaMalloc(&q, n * sizeof(T)) != cudaSuccess) {
+        cudaGetLastError();
+        return ISPAN_ERR_NOMEM;
+    }
+    owned.push_back(q);
+    *p = (T *)q;
+    return ISPAN_OK;
+}
+
+}  // namespace
+
+struct ispan_ctx {
+    int device = 0;
+    int nsm = 148;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int64_t maxV = 0, maxE = 0, maxW = 0;
+    int64_t maxSeg = 0;
+    std::vector<void *> owned;      // fixed scratch
+    std::vector<void *> seg_owned;  // per-segment arrays (grow on demand)
+    std::vector<void *> csr_owned;  // uploaded host graphs
+
+    // device scratch
+    int32_t *label = nullptr;
+    uint8_t *cls = nullptr;
+    uint32_t *A = nullptr, *F = nullptr, *B = nullptr, *D = nullptr, *P = nullptr;
+    int32_t *qv[2] = {nullptr, nullptr};
+    int64_t *qe[2] = {nullptr, nullptr};
+    int32_t *qchunk[2] = {nullptr, nullptr};
+    int32_t *wl[2] = {nullptr, nullptr};
+    int32_t *cnt_out = nullptr, *cnt_in = nullptr, *parent = nullptr, *aux = nullptr, *aux2 = nullptr,
+            *members = nullptr, *roots = nullptr, *small = nullptr, *large[2] = {nullptr, nullptr};
+    unsigned long long *ctlblk = nullptr;  // counters | qpk | lvl | ctl64
+    int64_t *hist = nullptr;
+    unsigned int *gsync = nullptr;
+    int *err = nullptr;
+    BfsCtl *bfsctl = nullptr;
+    int64_t *vbase = nullptr;
+    unsigned long long *pivot_key = nullptr, *gsize = nullptr;
+    int32_t *gmin = nullptr;
+
+    // uploaded CSR (host input)
+    void *up_fw_beg = nullptr, *up_bw_beg = nullptr;
+    int32_t *up_fw_adj = nullptr, *up_bw_adj = nullptr;
+    int64_t up_V = -1, up_E = -1;
+
+    // host staging
+    unsigned long long *h_counters = nullptr;  // pinned
+    int *h_err = nullptr;
+
+    // launch geometry
+    int g_stream = 0;           // grid for plain grid-stride kernels
+    int g_coop[4] = {0, 0, 0, 0};  // bfs<0>, bfs<1>, trim1, color (per offset width)
+    int g_coop_w = 0;           // offset width the coop grids were computed for
+
+    // CUDA graph cache
+    cudaGraphExec_t gexec = nullptr;
+    char gkey[256];
+    bool graph_broken = false;
+    cudaEvent_t ev[12];
+    bool have_ev = false;
+
+    // last run (for ispan_ref_codes)
+    int64_t last_V = 0;
+    int32_t *last_label = nullptr;
+    int64_t last_nseg = 1;
+    std::mutex mu;
+};
+
+static int64_t words_of(int64_t V) { return (V + 31) / 32 + 1; }
+
+static constexpr int kCtlCounters = 0;                       // kNumCounters
+static constexpr int kCtlQpk = kNumCounters;                 // 3
+static constexpr int kCtlLvl = kNumCounters + 4;             // 12
+static constexpr int kCtlX = kNumCounters + 4 + 16;          // kNumCtl
+static constexpr int kCtlTotal = kCtlX + kNumCtl;
+
+extern "C" int64_t ispan_ctx_bytes(int64_t V, int64_t E) {
+    int64_t W = words_of(V);
+    int64_t b = 0;
+    b += V * 4 + V;                 // label, cls
+    b += 5 * W * 4;                 // bitmaps
+    b += 2 * (V * 4 + (V + 1) * 8); // queues
+    b += 2 * ((E / kChunk + 4) * 4);
+    b += 2 * V * 4;                 // worklists
+    b += 10 * V * 4;                // counters, parent, aux, aux2, members, roots, small, large x2
+    b += (kHistCap + kBigCap) * 8;
+    return b;
+}
+
+static int ctx_alloc(ispan_ctx *c) {
+    int64_t V = c->maxV + 32, E = c->maxE;
+    int64_t W = words_of(V);
+    c->maxW = W;
+    int rc = 0;
+    auto &o = c->owned;
+    rc |= dalloc(&c->label, V, o);
+    rc |= dalloc(&c->cls, V, o);
+    rc |= dalloc(&c->A, W, o);
+    rc |= dalloc(&c->F, W, o);
+    rc |= dalloc(&c->B, W, o);
+    rc |= dalloc(&c->D, W, o);
+    rc |= dalloc(&c->P, W, o);
+    for (int i = 0; i < 2; ++i) {
+        rc |= dalloc(&c->qv[i], V, o);
+        rc |= dalloc(&c->qe[i], V + 1, o);
+        rc |= dalloc(&c->qchunk[i], E / kChunk + 4, o);
+        rc |= dalloc(&c->wl[i], V, o);
+        rc |= dalloc(&c->large[i], V, o);
+    }
+    rc |= dalloc(&c->cnt_out, V, o);
+    rc |= dalloc(&c->cnt_in, V, o);
+    rc |= dalloc(&c->parent, V, o);
+    rc |= dalloc(&c->aux, V, o);
+    rc |= dalloc(&c->aux2, V, o);
+    rc |= dalloc(&c->members, V, o);
+    rc |= dalloc(&c->roots, V, o);
+    rc |= dalloc(&c->small, V, o);
+    rc |= dalloc(&c->ctlblk, kCtlTotal, o);
+    rc |= dalloc(&c->hist, kHistCap + kBigCap, o);
+    rc |= dalloc(&c->gsync, 4, o);
+    rc |= dalloc(&c->err, 4, o);
+    rc |= dalloc(&c->bfsctl, 1, o);
+    return rc ? ISPAN_ERR_NOMEM : ISPAN_OK;
+}
+
+static int ctx_segments(ispan_ctx *c, int64_t nseg) {
+    if (nseg <= c->maxSeg) return ISPAN_OK;
+    for (void *p : c->seg_owned) cudaFree(p);
+    c->seg_owned.clear();
+    int64_t n = std::max<int64_t>(nseg, 1);
+    int rc = 0;
+    rc |= dalloc(&c->vbase, n + 1, c->seg_owned);
+    rc |= dalloc(&c->pivot_key, n, c->seg_owned);
+    rc |= dalloc(&c->gsize, n, c->seg_owned);
+    rc |= dalloc(&c->gmin, n, c->seg_owned);
+    if (rc) {
+        c->maxSeg = 0;
+        return ISPAN_ERR_NOMEM;
+    }
+    c->maxSeg = n;
+    if (c->gexec) {
+        cudaGraphExecDestroy(c->gexec);
+        c->gexec = nullptr;
+    }
+    return ISPAN_OK;
+}
+
+template <typename K>
+static int coop_grid(K kernel, int nsm, int block) {
+    int per = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, block, 0) != cudaSuccess || per < 1) {
+        cudaGetLastError();
+        return 0;
+    }
+    return per * nsm;
+}
+
+template <typename OffT>
+static void fill_run(ispan_ctx *c, Run<OffT> &r, Ext<OffT> &x, int64_t V, int64_t E, int32_t nseg,
+                     const OffT *fwb, const OffT *bwb, const int32_t *fwa, const int32_t *bwa, int32_t *label,
+                     const ispan_params *p) {
+    r.V = V;
+    r.E = E;
+    r.W = (V + 31) / 32;
+    r.nseg = nseg;
+    r.vbase = c->vbase;
+    r.fw_beg = fwb;
+    r.bw_beg = bwb;
+    r.fw_adj = fwa;
+    r.bw_adj = bwa;
+    r.label = label;
+    r.A = c->A; r.F = c->F; r.B = c->B; r.D = c->D; r.P = c->P;
+    for (int i = 0; i < 2; ++i) {
+        r.qv[i] = c->qv[i];
+        r.qe[i] = c->qe[i];
+        r.qchunk[i] = c->qchunk[i];
+        r.wl[i] = c->wl[i];
+    }
+    r.qpk = c->ctlblk + kCtlQpk;
+    r.lvl = c->ctlblk + kCtlLvl;
+    r.wlc = nullptr;
+    r.cnt_out = c->cnt_out;
+    r.cnt_in = c->cnt_in;
+    r.parent = c->parent;
+    r.aux = c->aux;
+    r.aux2 = c->aux2;
+    r.members = c->members;
+    r.pivot_key = c->pivot_key;
+    r.gmin = c->gmin;
+    r.gsize = c->gsize;
+    r.cls = c->cls;
+    r.counters = c->ctlblk + kCtlCounters;
+    r.hist = c->hist;
+    r.gsync = c->gsync;
+    r.err = c->err;
+    r.alpha = p && p->alpha > 0 ? p->alpha : 30;
+    r.beta = p && p->beta > 0 ? p->beta : 200;
+    r.gamma = p && p->gamma > 0 ? p->gamma : 10;
+    r.flags = p ? p->flags : 0;
+    x.ctl = c->ctlblk + kCtlX;
+    x.roots = c->roots;
+    x.small = c->small;
+    x.large[0] = c->large[0];
+    x.large[1] = c->large[1];
+    x.cq[0] = c->qv[0];  // the frontier queues are free once the giant is done
+    x.cq[1] = c->qv[1];
+}
+
+template <typename Kern, typename... Args>
+static cudaError_t launch_coop(Kern k, int grid, cudaStream_t s, Args... args) {
+    void *ptrs[] = {(void *)&args...};
+    return cudaLaunchCooperativeKernel((const void *)k, dim3(grid), dim3(kBlock), ptrs, 0, s);
+}
+
+// Enqueue the whole pipeline on c->stream (plain launches; may be captured).
+template <typename OffT>
+static cudaError_t enqueue(ispan_ctx *c, Run<OffT> r, Ext<OffT> x, bool times) {
+    cudaStream_t s = c->stream;
+    const int G = c->g_stream;
+    unsigned long long *ctl = c->ctlblk;
+    cudaError_t e;
+#define EV(i) \
+    if (times) { e = cudaEventRecord(c->ev[i], s); if (e) return e; }
+#define LK(...) \
+    do { __VA_ARGS__; e = cudaGetLastError(); if (e) return e; } while (0)
+    EV(0);
+    if ((e = cudaMemsetAsync(ctl, 0, kCtlTotal * sizeof(unsigned long long), s))) return e;
+    if ((e = cudaMemsetAsync(c->hist, 0, (kHistCap + kBigCap) * sizeof(int64_t), s))) return e;
+    if ((e = cudaMemsetAsync(c->gsync, 0, 4 * sizeof(unsigned), s))) return e;
+    if ((e = cudaMemsetAsync(c->err, 0, 4 * sizeof(int), s))) return e;
+    if ((e = cudaMemsetAsync(c->pivot_key, 0, r.nseg * sizeof(unsigned long long), s))) return e;
+    if ((e = cudaMemsetAsync(c->gsize, 0, r.nseg * sizeof(unsigned long long), s))) return e;
+    if ((e = cudaMemsetAsync(c->gmin, 0x7f, r.nseg * sizeof(int32_t), s))) return e;
+    LK((k_trim1_first<OffT><<<G, kBlock, 0, s>>>(r, x)));
+    EV(1);
+    LK((k_seed<OffT, 0><<<std::max<int64_t>(1, (r.nseg + 1023) / 1024), 32 * 32, 0, s>>>(r)));
+    if ((e = launch_coop(k_bfs<OffT, 0>, c->g_coop[0], s, r, c->bfsctl))) return e;
+    EV(2);
+    if ((e = cudaMemsetAsync(r.qpk, 0, 16 * sizeof(unsigned long long) + 4 * 8, s))) return e;
+    if ((e = cudaMemsetAsync(r.lvl, 0, 16 * sizeof(unsigned long long), s))) return e;
+    LK((k_seed<OffT, 1><<<std::max<int64_t>(1, (r.nseg + 1023) / 1024), 32 * 32, 0, s>>>(r)));
+    if ((e = launch_coop(k_bfs<OffT, 1>, c->g_coop[1], s, r, c->bfsctl))) return e;
+    EV(3);
+    LK((k_giant<OffT><<<G, kBlock, 0, s>>>(r, x)));
+    LK((k_residual<OffT><<<G, kBlock, 0, s>>>(r, x)));
+    EV(4);
+    if ((e = launch_coop(k_trim1<OffT>, c->g_coop[2], s, r, x, 0, 1))) return e;
+    EV(5);
+    LK((k_trim2<OffT><<<G, kBlock, 0, s>>>(r, x, 1)));
+    EV(6);
+    LK((k_trim3<OffT><<<G, kBlock, 0, s>>>(r, x, 1)));
+    EV(7);
+    if ((e = cudaMemsetAsync(x.ctl + K_CQ0, 0, 3 * sizeof(unsigned long long), s))) return e;
+    if ((e = cudaMemsetAsync(x.ctl + K_WL0, 0, sizeof(unsigned long long), s))) return e;
+    if ((e = launch_coop(k_trim1<OffT>, c->g_coop[2], s, r, x, 1, 0))) return e;
+    EV(8);
+    LK((k_wcc_init<OffT><<<G, kBlock, 0, s>>>(r, x, 0)));
+    LK((k_wcc_hook<OffT><<<G, kBlock, 0, s>>>(r, x, 0)));
+    LK((k_wcc_flatten<OffT><<<G, kBlock, 0, s>>>(r, x, 0)));
+    LK((k_wcc_alloc<OffT><<<G, kBlock, 0, s>>>(r, x)));
+    LK((k_wcc_scatter<OffT><<<G, kBlock, 0, s>>>(r, x, 0)));
+    EV(9);
+    LK((k_local_scc<OffT><<<c->nsm * 6, kLocalThreads, 0, s>>>(r, x)));
+    if ((e = launch_coop(k_color<OffT>, c->g_coop[3], s, r, x))) return e;
+    EV(10);
+    LK((k_finalize<OffT><<<G, kBlock, 0, s>>>(r, x)));
+    EV(11);
+#undef EV
+#undef LK
+    return cudaSuccess;
+}
+
+template <typename OffT>
+static int coop_setup(ispan_ctx *c) {
+    int w = (int)sizeof(OffT);
+    if (c->g_coop_w == w) return ISPAN_OK;
+    c->g_coop[0] = coop_grid(k_bfs<OffT, 0>, c->nsm, kBlock);
+    c->g_coop[1] = coop_grid(k_bfs<OffT, 1>, c->nsm, kBlock);
+    c->g_coop[2] = coop_grid(k_trim1<OffT>, c->nsm, kBlock);
+    c->g_coop[3] = coop_grid(k_color<OffT>, c->nsm, kBlock);
+    for (int i = 0; i < 4; ++i)
+        if (c->g_coop[i] < 1) return ISPAN_ERR_CUDA;
+    c->g_coop_w = w;
+    return ISPAN_OK;
+}
+
+template <typename OffT>
+static int run_t(ispan_ctx *c, int64_t V, int64_t E, int32_t nseg, const OffT *fwb, const OffT *bwb,
+                 const int32_t *fwa, const int32_t *bwa, int32_t *label_dev, const ispan_params *p,
+                 ispan_stats *st) {
+    int rc = coop_setup<OffT>(c);
+    if (rc) return rc;
+    Run<OffT> r;
+    Ext<OffT> x;
+    memset(&r, 0, sizeof(r));
+    memset(&x, 0, sizeof(x));
+    fill_run<OffT>(c, r, x, V, E, nseg, fwb, bwb, fwa, bwa, label_dev, p);
+    const uint32_t flags = p ? p->flags : 0;
+    const bool times = (flags & ISPAN_F_STAGE_TIMES) && st;
+    bool use_graph = !(flags & ISPAN_F_NO_GRAPH) && !c->graph_broken && !times;
+    if (use_graph) {
+        char key[256];
+        snprintf(key, sizeof key, "%d|%lld|%lld|%d|%p|%p|%p|%p|%p|%d|%d|%d|%d", (int)sizeof(OffT), (long long)V,
+                 (long long)E, nseg, (const void *)fwb, (const void *)bwb, (const void *)fwa, (const void *)bwa,
+                 (void *)label_dev, r.alpha, r.beta, r.gamma, (int)(uintptr_t)c->stream);
+        if (!c->gexec || strcmp(key, c->gkey) != 0) {
+            if (c->gexec) {
+                cudaGraphExecDestroy(c->gexec);
+                c->gexec = nullptr;
+            }
+            cudaGraph_t g = nullptr;
+            cudaError_t e = cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal);
+            if (e == cudaSuccess) {
+                cudaError_t e2 = enqueue<OffT>(c, r, x, false);
+                e = cudaStreamEndCapture(c->stream, &g);
+                if (e2 != cudaSuccess) e = e2;
+            }
+            if (e == cudaSuccess) e = cudaGraphInstantiate(&c->gexec, g, 0);
+            if (g) cudaGraphDestroy(g);
+            if (e != cudaSuccess) {
+                cudaGetLastError();
+                c->graph_broken = true;  // fall back to direct launches from now on
+                c->gexec = nullptr;
+                use_graph = false;
+            } else {
+                snprintf(c->gkey, sizeof c->gkey, "%s", key);
+            }
+        }
+    }
+    if (use_graph) {
+        CK(cudaGraphLaunch(c->gexec, c->stream));
+    } else {
+        CK(enqueue<OffT>(c, r, x, times));
+    }
+    CK(cudaMemcpyAsync(c->h_counters, c->ctlblk, kNumCounters * sizeof(unsigned long long),
+                       cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(c->h_err, c->err, 4 * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (c->h_err[0]) return c->h_err[0] < 0 ? c->h_err[0] : ISPAN_ERR_INTERNAL;
+    if (st) {
+        const unsigned long long *k = c->h_counters;
+        memset(st->stage_ms, 0, sizeof(st->stage_ms));
+        st->giant_size = (int64_t)k[C_GIANT];
+        st->n_trim1 = (int64_t)k[C_TRIM1];
+        st->n_trim2 = (int64_t)k[C_TRIM2];
+        st->n_trim3 = (int64_t)k[C_TRIM3];
+        st->n_mice_vertices = (int64_t)k[C_MICE_V];
+        st->n_mice_scc = (int64_t)k[C_MICE_SCC];
+        st->n_wcc = (int64_t)k[C_WCC];
+        st->fw_size = (int64_t)k[C_FW_SIZE];
+        st->fw_levels = (int64_t)k[C_FW_LEVELS];
+        st->bw_levels = (int64_t)k[C_BW_LEVELS];
+        st->color_rounds = (int64_t)k[C_COLOR_ROUNDS];
+        st->local_wcc = (int64_t)k[C_LOCAL_WCC];
+        st->trim_rounds = (int64_t)k[C_TRIM_ROUNDS];
+        st->residual = 0;
+        st->scc_count = (int64_t)(k[C_TRIM1] + k[C_TRIM2] / 2 + k[C_TRIM3] / 3 + k[C_MICE_SCC] + k[C_GIANTS]);
+        if (times) {
+            float ms[12];
+            for (int i = 1; i < 12; ++i) cudaEventElapsedTime(&ms[i], c->ev[i - 1], c->ev[i]);
+            // reference slots: 0 trim, 1 elephant, 2 mice, 3 total, 4 trim size_1,
+            // 5 trim size_2, 6 pivot, 7 fw, 8 bw, 9 wcc, 10 mice fw-bw, 13 trim size_3
+            st->stage_ms[6] = ms[1];
+            st->stage_ms[7] = ms[2];
+            st->stage_ms[8] = ms[3];
+            st->stage_ms[4] = ms[1] + ms[4] + ms[5] + ms[8];
+            st->stage_ms[5] = ms[6];
+            st->stage_ms[13] = ms[7];
+            st->stage_ms[9] = ms[9];
+            st->stage_ms[10] = ms[10];
+            st->stage_ms[0] = st->stage_ms[4] + st->stage_ms[5] + st->stage_ms[13];
+            st->stage_ms[1] = ms[2] + ms[3];
+            st->stage_ms[2] = ms[9] + ms[10];
+            float tot = 0;
+            cudaEventElapsedTime(&tot, c->ev[0], c->ev[11]);
+            st->stage_ms[3] = tot;
+        }
+        st->hist_n = 0;
+        if (st->hist_size && st->hist_count && st->hist_cap > 0) {
+            std::vector<int64_t> h(kHistCap + kBigCap);
+            CK(cudaMemcpy(h.data(), c->hist, h.size() * sizeof(int64_t), cudaMemcpyDeviceToHost));
+            std::vector<std::pair<int64_t, int64_t>> pairs;
+            for (int i = 1; i < kHistCap; ++i)
+                if (h[i]) pairs.push_back({i, h[i]});
+            int64_t nbig = std::min<int64_t>((int64_t)k[C_BIG], kBigCap);
+            std::vector<int64_t> big(h.begin() + kHistCap, h.begin() + kHistCap + nbig);
+            std::sort(big.begin(), big.end());
+            for (size_t i = 0; i < big.size();) {
+                size_t j = i;
+                while (j < big.size() && big[j] == big[i]) ++j;
+                pairs.push_back({big[i], (int64_t)(j - i)});
+                i = j;
+            }
+            st->hist_n = (int64_t)pairs.size();
+            for (int64_t i = 0; i < st->hist_n && i < st->hist_cap; ++i) {
+                st->hist_size[i] = pairs[i].first;
+                st->hist_count[i] = pairs[i].second;
+            }
+        }
+    }
+    c->last_V = V;
+    c->last_label = label_dev;
+    c->last_nseg = nseg;
+    return ISPAN_OK;
+}
+
+static int check_csr(const ispan_csr *g) {
+    if (!g || g->V < 0 || g->E < 0) return ISPAN_ERR_ARG;
+    if (g->offset_bytes != 4 && g->offset_bytes != 8) return ISPAN_ERR_ARG;
+    if (g->offset_bytes == 4 && g->E > INT32_MAX) return ISPAN_ERR_ARG;
+    if (g->V >= INT32_MAX) return ISPAN_ERR_ARG;
+    if (g->V > 0 && (!g->fw_beg || !g->bw_beg)) return ISPAN_ERR_ARG;
+    if (g->E > 0 && (!g->fw_adj || !g->bw_adj)) return ISPAN_ERR_ARG;
+    return ISPAN_OK;
+}
+
+// host offsets are validated before upload: monotone, 0..E
+static int check_host_offsets(const ispan_csr *g) {
+    for (int k = 0; k < 2; ++k) {
+        const void *b = k ? g->bw_beg : g->fw_beg;
+        int64_t prev = 0;
+        for (int64_t i = 0; i <= g->V; ++i) {
+            int64_t x = g->offset_bytes == 4 ? ((const int32_t *)b)[i] : ((const int64_t *)b)[i];
+            if ((i == 0 && x != 0) || x < prev) return ISPAN_ERR_ARG;
+            prev = x;
+        }
+        if (prev != g->E) return ISPAN_ERR_ARG;
+    }
+    return ISPAN_OK;
+}
+
+static int upload(ispan_ctx *c, const ispan_csr *g) {
+    size_t ob = (size_t)g->offset_bytes;
+    if (c->up_V < g->V || c->up_E < g->E || c->up_fw_beg == nullptr) {
+        for (void *p : c->csr_owned) cudaFree(p);
+        c->csr_owned.clear();
+        int rc = 0;
+        char *a = nullptr, *b = nullptr;
+        rc |= dalloc(&a, (size_t)(g->V + 1) * 8, c->csr_owned);
+        rc |= dalloc(&b, (size_t)(g->V + 1) * 8, c->csr_owned);
+        rc |= dalloc(&c->up_fw_adj, (size_t)g->E, c->csr_owned);
+        rc |= dalloc(&c->up_bw_adj, (size_t)g->E, c->csr_owned);
+        if (rc) {
+            c->up_V = c->up_E = -1;
+            c->up_fw_beg = nullptr;
+            return ISPAN_ERR_NOMEM;
+        }
+        c->up_fw_beg = a;
+        c->up_bw_beg = b;
+        c->up_V = g->V;
+        c->up_E = g->E;
+    }
+    CK(cudaMemcpyAsync(c->up_fw_beg, g->fw_beg, (size_t)(g->V + 1) * ob, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->up_bw_beg, g->bw_beg, (size_t)(g->V + 1) * ob, cudaMemcpyHostToDevice, c->stream));
+    if (g->E) {
+        CK(cudaMemcpyAsync(c->up_fw_adj, g->fw_adj, (size_t)g->E * 4, cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(c->up_bw_adj, g->bw_adj, (size_t)g->E * 4, cudaMemcpyHostToDevice, c->stream));
+    }
+    return ISPAN_OK;
+}
+
+static int run_common(ispan_ctx *c, const ispan_csr *g, int32_t nseg, const int64_t *vbase_host,
+                      const ispan_params *p, int32_t *labels_out, ispan_stats *st) {
+    if (!c) return ISPAN_ERR_ARG;
+    int rc = check_csr(g);
+    if (rc) return rc;
+    if (g->V > c->maxV || g->E > c->maxE) return ISPAN_ERR_CAPACITY;
+    if (nseg < 1) return ISPAN_ERR_ARG;
+    std::lock_guard<std::mutex> lock(c->mu);
+    if (cudaSetDevice(c->device) != cudaSuccess) return ISPAN_ERR_CUDA;
+    if ((rc = ctx_segments(c, nseg))) return rc;
+    std::vector<int64_t> vb;
+    if (vbase_host) {
+        vb.assign(vbase_host, vbase_host + nseg + 1);
+        if (vb[0] != 0 || vb[nseg] != g->V) return ISPAN_ERR_ARG;
+        for (int i = 0; i < nseg; ++i)
+            if (vb[i + 1] < vb[i]) return ISPAN_ERR_ARG;
+    } else {
+        vb = {0, g->V};
+    }
+    CK(cudaMemcpyAsync(c->vbase, vb.data(), vb.size() * sizeof(int64_t), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));  // vb is a host temporary
+    const void *fwb = g->fw_beg, *bwb = g->bw_beg;
+    const int32_t *fwa = g->fw_adj, *bwa = g->bw_adj;
+    if (!g->on_device) {
+        if ((rc = check_host_offsets(g))) return rc;
+        if ((rc = upload(c, g))) return rc;
+        fwb = c->up_fw_beg;
+        bwb = c->up_bw_beg;
+        fwa = c->up_fw_adj;
+        bwa = c->up_bw_adj;
+    }
+    const bool dev_labels = p && (p->flags & ISPAN_F_LABELS_ON_DEVICE);
+    int32_t *label = dev_labels ? labels_out : c->label;
+    if (!label && g->V) return ISPAN_ERR_ARG;
+    if (g->offset_bytes == 4)
+        rc = run_t<int32_t>(c, g->V, g->E, nseg, (const int32_t *)fwb, (const int32_t *)bwb, fwa, bwa, label, p, st);
+    else
+        rc = run_t<int64_t>(c, g->V, g->E, nseg, (const int64_t *)fwb, (const int64_t *)bwb, fwa, bwa, label, p, st);
+    if (rc) return rc;
+    if (!dev_labels && labels_out && g->V) {
+        CK(cudaMemcpyAsync(labels_out, c->label, (size_t)g->V * 4, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+    }
+    return ISPAN_OK;
+}
+
+extern "C" {
+
+int ispan_ctx_create(int device, int64_t max_V, int64_t max_E, ispan_ctx **out) {
+    if (!out || max_V < 0 || max_E < 0 || max_V >= INT32_MAX) return ISPAN_ERR_ARG;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return ISPAN_ERR_NODEV;
+    }
+    if (device < 0 || device >= ndev) return ISPAN_ERR_ARG;
+    if (cudaSetDevice(device) != cudaSuccess) return ISPAN_ERR_CUDA;
+    ispan_ctx *c = new ispan_ctx();
+    c->device = device;
+    c->maxV = max_V;
+    c->maxE = max_E;
+    cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, device);
+    int rc = ctx_alloc(c);
+    if (!rc) rc = ctx_segments(c, 1);
+    if (!rc && cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) rc = ISPAN_ERR_CUDA;
+    c->own_stream = true;
+    if (!rc && cudaMallocHost(&c->h_counters, kNumCounters * sizeof(unsigned long long)) != cudaSuccess)
+        rc = ISPAN_ERR_NOMEM;
+    if (!rc && cudaMallocHost(&c->h_err, 4 * sizeof(int)) != cudaSuccess) rc = ISPAN_ERR_NOMEM;
+    if (!rc) {
+        for (int i = 0; i < 12; ++i)
+            if (cudaEventCreate(&c->ev[i]) != cudaSuccess) rc = ISPAN_ERR_CUDA;
+        c->have_ev = rc == 0;
+    }
+    int per = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_trim1_first<int64_t>, kBlock, 0);
+    c->g_stream = std::max(1, per) * c->nsm;
+    if (rc) {
+        cudaGetLastError();
+        ispan_ctx_destroy(c);
+        return rc;
+    }
+    *out = c;
+    return ISPAN_OK;
+}
+
+int ispan_ctx_destroy(ispan_ctx *c) {
+    if (!c) return ISPAN_OK;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->gexec) cudaGraphExecDestroy(c->gexec);
+    for (void *p : c->owned) cudaFree(p);
+    for (void *p : c->seg_owned) cudaFree(p);
+    for (void *p : c->csr_owned) cudaFree(p);
+    if (c->have_ev)
+        for (int i = 0; i < 12; ++i) cudaEventDestroy(c->ev[i]);
+    if (c->h_counters) cudaFreeHost(c->h_counters);
+    if (c->h_err) cudaFreeHost(c->h_err);
+    if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return ISPAN_OK;
+}
+
+int ispan_ctx_set_stream(ispan_ctx *c, void *stream) {
+    if (!c) return ISPAN_ERR_ARG;
+    std::lock_guard<std::mutex> lock(c->mu);
+    if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+    c->stream = (cudaStream_t)stream;
+    c->own_stream = false;
+    if (c->gexec) {
+        cudaGraphExecDestroy(c->gexec);
+        c->gexec = nullptr;
+    }
+    return ISPAN_OK;
+}
+
+int ispan_scc_run(ispan_ctx *c, const ispan_csr *g, const ispan_params *p, int32_t *labels_out,
+                  ispan_stats *st) {
+    return run_common(c, g, 1, nullptr, p, labels_out, st);
+}
+
+int ispan_scc_run_batch(ispan_ctx *c, const ispan_csr *g, int32_t nseg, const int64_t *vbase,
+                        const ispan_params *p, int32_t *labels_out, ispan_stats *st) {
+    if (!vbase) return ISPAN_ERR_ARG;
+    return run_common(c, g, nseg, vbase, p, labels_out, st);
+}
+
+int ispan_ref_codes(ispan_ctx *c, int32_t *codes) {
+    if (!c || !codes) return ISPAN_ERR_ARG;
+    std::lock_guard<std::mutex> lock(c->mu);
+    int64_t V = c->last_V;
+    std::vector<int32_t> lab(V);
+    std::vector<uint8_t> cls(V);
+    if (V) {
+        CK(cudaMemcpy(lab.data(), c->last_label, V * 4, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(cls.data(), c->cls, V, cudaMemcpyDeviceToHost));
+    }
+    for (int64_t v = 0; v < V; ++v) {
+        switch (cls[v]) {
+            case CLS_GIANT: codes[v] = 1; break;
+            case CLS_TRIM1: codes[v] = -1; break;
+            case CLS_TRIM2: codes[v] = -2; break;
+            case CLS_TRIM3: codes[v] = -3; break;
+            default: codes[v] = lab[v] + 2; break;
+        }
+    }
+    codes[V] = 0;
+    return ISPAN_OK;
+}
+
+const char *ispan_strerror(int code) {
+    switch (code) {
+        case ISPAN_OK: return "ok";
+        case ISPAN_ERR_ARG: return "bad argument or malformed CSR";
+        case ISPAN_ERR_NOMEM: return "device allocation failed";
+        case ISPAN_ERR_CUDA: return "CUDA runtime error";
+        case ISPAN_ERR_TIMEOUT: return "device-side wait timed out";
+        case ISPAN_ERR_INTERNAL: return "internal device-side check failed";
+        case ISPAN_ERR_NODEV: return "no CUDA device";
+        case ISPAN_ERR_CAPACITY: return "graph exceeds the context's capacity";
+        default: return "unknown error";
+    }
+}
+
+const char *ispan_version(void) { return "ispan_b200 0.1 (sm_100a)"; }
+
+}  // extern "C"

@@ -1,0 +1,881 @@
+// stages.cuh -- every stage of the pipeline except the reachability
+// searches (bfs.cuh).  Each kernel cites the reference function it replaces.
+//
+// Soundness of the concurrent trims: a trim kernel claims a vertex set only
+// when the set is strongly connected through static edges and closed (in one
+// edge direction) over the vertices it observed as still active.  Vertices
+// only ever leave the active map, and only as whole true SCCs, so an
+// observation "x is inactive" always means x belongs to another, already
+// final SCC -- unless a concurrent claim of a *larger* set is in flight.
+// Kernels therefore never mix claim sizes: trim-2 and trim-3 run as separate
+// launches, and the peel (trim-1) decides from counters, not observations.
+#pragma once
+#include "common.cuh"
+
+namespace ispan {
+
+// classes recorded per vertex (for the reference-convention codes)
+enum Cls : uint8_t { CLS_NONE = 0, CLS_GIANT = 1, CLS_TRIM1 = 2, CLS_TRIM2 = 3, CLS_TRIM3 = 4, CLS_MICE = 5 };
+
+// control-block slots (Run::ctl64): worklist and queue counters
+enum Ctl64 {
+    K_WL0 = 0, K_WL1, K_CQ0, K_CQ1, K_CQ2, K_ROOTS, K_SMALL, K_LARGE, K_ALLOC, K_LARGE2,
+    K_SPILL, K_MICE_SCC, kNumCtl = 32
+};
+
+constexpr int kLocalV = 1024;   // a WCC up to this many vertices ...
+constexpr int kLocalE = 4096;   // ... and internal edges is solved in shared memory
+
+template <typename OffT>
+struct Ext {
+    unsigned long long *ctl;      // [kNumCtl]
+    int32_t *roots;               // [V] WCC roots
+    int32_t *small;               // [V] small WCC roots
+    int32_t *large[2];            // [V] vertices of large WCCs (double buffered)
+    int32_t *cq[2];               // [V] peel cascade queues
+};
+
+// ---------------------------------------------------------------------------
+// Block-level compaction of bitmap words into a worklist with one atomic per
+// CTA: the CTA owns a contiguous range of words, counts, reserves, then
+// writes its vertices in word order.
+template <typename WordFn>
+__device__ void compact_words(int64_t W, WordFn f, int32_t *out, unsigned long long *cnt) {
+    __shared__ int64_t sh[kWarps];
+    __shared__ int s_warp[kWarps];
+    __shared__ unsigned long long s_base;
+    const int warp = threadIdx.x >> 5, lane = lane_id();
+    int64_t per = (W + gridDim.x - 1) / gridDim.x;
+    int64_t w0 = min(W, (int64_t)blockIdx.x * per), w1 = min(W, w0 + per);
+    int64_t mine = 0;
+    for (int64_t wi = w0 + threadIdx.x; wi < w1; wi += kBlock) mine += __popc(f(wi));
+    int64_t tot = block_sum64(mine, sh);
+    if (threadIdx.x == 0) s_base = tot ? atomicAdd(cnt, (unsigned long long)tot) : 0;
+    __syncthreads();
+    int64_t run = (int64_t)s_base;
+    for (int64_t wb = w0; wb < w1; wb += kWarps) {
+        int64_t wi = wb + warp;
+        uint32_t m = (wi < w1) ? f(wi) : 0u;  // every lane evaluates; same value
+        if (lane == 0) s_warp[warp] = __popc(m);
+        __syncthreads();
+        int off = 0, all = 0;
+        for (int i = 0; i < kWarps; ++i) {
+            if (i < warp) off += s_warp[i];
+            all += s_warp[i];
+        }
+        if ((m >> lane) & 1u) out[run + off + __popc(m & lanemask_lt())] = (int32_t)(wi * 32 + lane);
+        run += all;
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// trim_1_first (src/trim_1_gfq.h:9-33) fused with generate_frontier_queue's
+// bookkeeping (:486-529) and pivot_selection_from_fq (src/scc_common.h:92-150):
+// one pass over the offsets.  A vertex with zero full out- or in-degree is its
+// own SCC; the rest form the active map.  Pivot key per graph:
+// (min(outdeg*indeg, 2^32-1) << 32) | ~id, i.e. the largest degree product,
+// ties to the lowest id, in 64-bit arithmetic (the reference's int32 product
+// overflows on hubs).
+template <typename OffT>
+__global__ void __launch_bounds__(kBlock) k_trim1_first(Run<OffT> r, Ext<OffT> x) {
+    __shared__ int64_t sh[kWarps];
+    const int lane = lane_id();
+    const int64_t gw = ((int64_t)blockIdx.x * kBlock + threadIdx.x) >> 5;
+    const int64_t nw = (int64_t)gridDim.x * kWarps;
+    int64_t n_act = 0, mu = 0, n_tr = 0;
+    unsigned long long best = 0;
+    for (int64_t wi = gw; wi < r.W; wi += nw) {
+        int64_t v = wi * 32 + lane;
+        bool valid = v < r.V;
+        int64_t od = 0, id = 0;
+        if (valid) {
+            od = ld_off(r.fw_beg, v + 1) - ld_off(r.fw_beg, v);
+            id = ld_off(r.bw_beg, v + 1) - ld_off(r.bw_beg, v);
+        }
+        bool act = valid && od > 0 && id > 0;
+        unsigned am = __ballot_sync(kFull, act);
+        if (lane == 0) {
+            r.A[wi] = am;
+            r.F[wi] = 0;
+            r.B[wi] = 0;
+            r.D[wi] = 0;
+        }
+        if (valid && !act) {
+            r.label[v] = (int32_t)v;
+            r.cls[v] = CLS_TRIM1;
+            ++n_tr;
+        }
+        unsigned long long key = 0;
+        if (act) {
+            ++n_act;
+            mu += od;
+            unsigned long long prod = (unsigned long long)od * (unsigned long long)id;
+            if (prod > 0xffffffffull) prod = 0xffffffffull;
+            key = (prod << 32) | (0xffffffffull - (unsigned long long)v);
+        }
+        if (r.nseg == 1) {
+            best = key > best ? key : best;
+        } else {
+            // segmented: lanes of one word nearly always share a graph
+            int s = valid ? seg_of(r.vbase, r.nseg, v) : -1;
+            int s0 = __shfl_sync(kFull, s, 0);
+            bool uni = __all_sync(kFull, s == s0 || s < 0);
+            if (uni) {
+                unsigned long long m = warp_max_u64(key);
+                if (lane == 0 && m) atomicMax(r.pivot_key + s0, m);
+            } else if (key) {
+                atomicMax(r.pivot_key + s, key);
+            }
+        }
+    }
+    if (r.nseg == 1) {
+        best = warp_max_u64(best);
+        if (lane == 0 && best) atomicMax(r.pivot_key, best);
+    }
+    int64_t a = block_sum64(n_act, sh), m = block_sum64(mu, sh), t = block_sum64(n_tr, sh);
+    if (threadIdx.x == 0) {
+        if (a) atomicAdd(r.counters + C_ACTIVE0, (unsigned long long)a);
+        if (m) atomicAdd(r.counters + C_MU0, (unsigned long long)m);
+        if (t) atomicAdd(r.counters + C_TRIM1, (unsigned long long)t);
+    }
+}
+
+// Seed the forward (DIR 0) or backward (DIR 1) search with each graph's
+// pivot: mark it, queue it at level 0.  Warp per 32 graphs.
+template <typename OffT, int DIR>
+__global__ void k_seed(Run<OffT> r) {
+    const int lane = lane_id();
+    int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int64_t nwp = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t b = gw * 32; b < r.nseg; b += nwp * 32) {
+        int64_t s = b + lane;
+        unsigned long long key = s < r.nseg ? r.pivot_key[s] : 0ull;
+        bool ok = key != 0;
+        int64_t p = ok ? (int64_t)(0xffffffffull - (key & 0xffffffffull)) : 0;
+        int64_t dg = 0, other = 0;
+        if (ok) {
+            if (DIR == 0) {
+                set_bit(r.F, p);
+                dg = ld_off(r.fw_beg, p + 1) - ld_off(r.fw_beg, p);
+                other = ld_off(r.bw_beg, p + 1) - ld_off(r.bw_beg, p);
+                atomicAdd(r.counters + C_FW_SIZE, 1ull);
+                atomicAdd(r.counters + C_FW_MU, (unsigned long long)other);
+            } else {
+                set_bit(r.B, p);
+                dg = ld_off(r.bw_beg, p + 1) - ld_off(r.bw_beg, p);
+            }
+        }
+        q_append(ok, (int32_t)p, dg, r.qv[0], r.qe[0], r.qchunk[0], r.qpk, r.V);
+    }
+}
+
+// The pivot SCC of each graph is B (reached backward inside F).  Leave the
+// active map, record the class, and find each graph's minimum member id (its
+// canonical label, written by k_finalize).  Warp per word.
+template <typename OffT>
+__global__ void __launch_bounds__(kBlock) k_giant(Run<OffT> r, Ext<OffT> x) {
+    __shared__ int64_t sh[kWarps];
+    const int lane = lane_id();
+    const int64_t gw = ((int64_t)blockIdx.x * kBlock + threadIdx.x) >> 5;
+    const int64_t nw = (int64_t)gridDim.x * kWarps;
+    int64_t n = 0;
+    int gm = 0x7fffffff;
+    for (int64_t wi = gw; wi < r.W; wi += nw) {
+        uint32_t s = r.B[wi];
+        if (!s) continue;
+        if (lane == 0) r.A[wi] &= ~s;
+        int64_t v = wi * 32 + lane;
+        bool me = (s >> lane) & 1u;
+        if (me) {
+            r.cls[v] = CLS_GIANT;
+            ++n;
+        }
+        if (r.nseg == 1) {
+            gm = min(gm, me ? (int)v : 0x7fffffff);
+        } else {
+            int sg = me ? seg_of(r.vbase, r.nseg, v) : -1;
+            unsigned grp = __match_any_sync(kFull, sg);
+            if (me) {
+                atomicMin(r.gmin + sg, (int)v);
+                if (lane == __ffs(grp) - 1) atomicAdd(r.gsize + sg, (unsigned long long)__popc(grp));
+            }
+        }
+    }
+    if (r.nseg == 1) {
+        gm = warp_min(gm);
+        if (lane == 0 && gm != 0x7fffffff) atomicMin(r.gmin, gm);
+    }
+    int64_t t = block_sum64(n, sh);
+    if (threadIdx.x == 0 && t) {
+        atomicAdd(r.counters + C_GIANT, (unsigned long long)t);
+        if (r.nseg == 1) atomicAdd(r.gsize, (unsigned long long)t);
+    }
+}
+
+// Residual worklist: every still-active vertex, in id order per CTA.
+template <typename OffT>
+__global__ void __launch_bounds__(kBlock) k_residual(Run<OffT> r, Ext<OffT> x) {
+    const uint32_t *A = r.A;
+    compact_words(r.W, [A] __device__(int64_t wi) { return A[wi]; }, r.wl[0], x.ctl + K_WL0);
+}
+
+// ---------------------------------------------------------------------------
+// trim_1_from_fq_gfq (src/trim_1_gfq.h:365-458) and its loops
+// (src/scc_core.cpp:562-602, :757-795), run to a fixpoint in one persistent
+// kernel: count each worklist vertex's active non-self in/out edges once,
+// then peel with a cascade -- a vertex whose last active out- (or in-)
+// neighbour is peeled reaches a zero counter and is peeled in the next round.
+// Work is proportional to the edges of the peeled vertices, not to
+// (passes x residual edges).  Survivors are compacted into the other worklist.
+template <typename OffT>
+__device__ __forceinline__ void count_active(const OffT *beg, const int32_t *adj, const uint32_t *A, int64_t v,
+                                             int32_t &n) {
+    int64_t e0 = ld_off(beg, v), e1 = ld_off(beg, v + 1);
+    int c = 0;
+    for (int64_t e = e0; e < e1; ++e) {
+        int32_t w = __ldg(adj + e);
+        c += (w != v) && bitc(A, w);
+    }
+    n = c;
+}
+
+template <typename OffT>
+__global__ void __launch_bounds__(kBlock) k_trim1(Run<OffT> r, Ext<OffT> x, int in, int out) {
+    __shared__ int64_t sh[kWarps];
+    const int64_t gt = (int64_t)blockIdx.x * kBlock + threadIdx.x;
+    const int64_t nt = (int64_t)gridDim.x * kBlock;
+    const int32_t *wl = r.wl[in];
+    const int64_t n = (int64_t)__ldcg(x.ctl + K_WL0 + in);
+    unsigned long long *cqc = x.ctl + K_CQ0;  // 3 rotating counters
+    // phase 1: counts against the active map as it stands (nothing is
+    // cleared until the barrier, so the counts are exact)
+    for (int64_t i = gt; i - (threadIdx.x) < n; i += nt) {
+        bool dead = false;
+        int32_t v = 0;
+        if (i < n) {
+            v = wl[i];
+            if (bitc(r.A, v)) {
+                int32_t o, ii;
+                count_active(r.fw_beg, r.fw_adj, r.A, v, o);
+                count_active(r.bw_beg, r.bw_adj, r.A, v, ii);
+                if (o == 0 || ii == 0) {
+                    dead = set_bit(r.D, v);
+                } else {
+                    r.cnt_out[v] = o;
+                    r.cnt_in[v] = ii;
+                }
+            }
+        }
+        wl_append(dead, v, x.cq[0], cqc + 0);
+    }
+    if (!grid_sync(r.gsync, r.err)) return;
+    // cascade rounds
+    int lv = 0;
+    for (int guard = 0; guard < (1 << 30); ++guard) {
+        const int c = lv & 1;
+        const int64_t m = (int64_t)__ldcg(cqc + lv % 3);
+        if (m == 0) break;
+        if (blockIdx.x == 0 && threadIdx.x == 0) cqc[(lv + 2) % 3] = 0ull;
+        const int32_t *q = x.cq[c];
+        for (int64_t i = gt; i - threadIdx.x < m; i += nt) {
+            int32_t t = i < m ? __ldcg(q + i) : 0;
+            bool live = i < m;
+            // out-edges t->w lower w's in-count; in-edges u->t lower u's out-count
+            for (int dir = 0; dir < 2; ++dir) {
+                const OffT *beg = dir == 0 ? r.fw_beg : r.bw_beg;
+                const int32_t *adj = dir == 0 ? r.fw_adj : r.bw_adj;
+                int32_t *cnt = dir == 0 ? r.cnt_in : r.cnt_out;
+                int64_t e0 = live ? ld_off(beg, t) : 0, e1 = live ? ld_off(beg, t + 1) : 0;
+                // edges one by one; appends are warp-aggregated per step
+                int64_t len = e1 - e0;
+                int64_t maxlen = len;
+                for (int o = 16; o; o >>= 1) maxlen = max(maxlen, __shfl_xor_sync(kFull, maxlen, o));
+                for (int64_t k = 0; k < maxlen; ++k) {
+                    bool nd = false;
+                    int32_t w = 0;
+                    if (k < len) {
+                        w = __ldg(adj + e0 + k);
+                        if (w != t && bitc(r.A, w) && !bitv(r.D, w)) {
+                            if (atomicSub(cnt + w, 1) == 1) nd = set_bit(r.D, w);
+                        }
+                    }
+                    wl_append(nd, w, x.cq[c ^ 1], cqc + (lv + 1) % 3);
+                }
+            }
+        }
+        if (!grid_sync(r.gsync, r.err)) return;
+        ++lv;
+    }
+    // final: peeled vertices leave; survivors move to the other worklist
+    int64_t peeled = 0;
+    for (int64_t i = gt; i - threadIdx.x < n; i += nt) {
+        bool keep = false;
+        int32_t v = 0;
+        if (i < n) {
+            v = wl[i];
+            if (bitc(r.A, v)) {
+                if (bitv(r.D, v)) {
+                    clear_bit(r.A, v);
+                    r.label[v] = v;
+                    r.cls[v] = CLS_TRIM1;
+                    ++peeled;
+                } else {
+                    keep = true;
+                }
+            }
+        }
+        wl_append(keep, v, r.wl[out], x.ctl + K_WL0 + out);
+    }
+    int64_t tp = block_sum64(peeled, sh);
+    if (threadIdx.x == 0) {
+        if (tp) atomicAdd(r.counters + C_TRIM1, (unsigned long long)tp);
+        if (blockIdx.x == 0) atomicAdd(r.counters + C_TRIM_ROUNDS, (unsigned long long)(lv + 1));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// trim-2 / trim-3 pattern checks.  distinct_active: up to `cap` distinct
+// active neighbours of v in one direction, skipping x1 and x2.
+template <typename OffT>
+__device__ __forceinline__ int distinct_active(const OffT *beg, const int32_t *adj, const uint32_t *A, int64_t v,
+                                               int32_t x1, int32_t x2, int cap, int32_t &n1, int32_t &n2) {
+    int64_t e0 = ld_off(beg, v), e1 = ld_off(beg, v + 1);
+    int d = 0;
+    for (int64_t e = e0; e < e1; ++e) {
+        int32_t w = __ldg(adj + e);
+        if (w == x1 || w == x2 || !bitv(A, w)) continue;
+        if (d == 0) { n1 = w; d = 1; }
+        else if (d == 1 && w != n1) { n2 = w; d = 2; }
+        else if (d == 2 && w != n1 && w != n2) { d = 3; }
+        if (d >= cap) break;
+    }
+    return d;
+}
+
+template <typename OffT>
+__device__ __forceinline__ bool claim(Run<OffT> &r, Ext<OffT> &x, int32_t v, int32_t lab, uint8_t cls) {
+    if (!set_bit(r.D, v)) return false;
+    r.label[v] = lab;
+    r.cls[v] = cls;
+    clear_bit(r.A, v);
+    return true;
+}
+
+// trim_2_from_fq (src/trim_2_3.h:146-283): sink 2-cycles (the vertex's only
+// active successor has the vertex as its only active successor) and source
+// 2-cycles (the same over predecessors).  Label = min of the pair.
+template <typename OffT>
+__global__ void __launch_bounds__(kBlock) k_trim2(Run<OffT> r, Ext<OffT> x, int in) {
+    __shared__ int64_t sh[kWarps];
+    const int64_t n = (int64_t)__ldcg(x.ctl + K_WL0 + in);
+    const int32_t *wl = r.wl[in];
+    int64_t got = 0;
+    for (int64_t i = (int64_t)blockIdx.x * kBlock + threadIdx.x; i < n; i += (int64_t)gridDim.x * kBlock) {
+        int32_t v = wl[i];
+        if (!bitv(r.A, v)) continue;
+        for (int dir = 0; dir < 2; ++dir) {
+            const OffT *beg = dir == 0 ? r.fw_beg : r.bw_beg;
+            const int32_t *adj = dir == 0 ? r.fw_adj : r.bw_adj;
+            int32_t a = -1, b = -1, c = -1, dd = -1;
+            if (distinct_active(beg, adj, r.A, v, v, v, 2, a, b) != 1) continue;
+            if (distinct_active(beg, adj, r.A, a, a, a, 2, c, dd) != 1 || c != v) continue;
+            int32_t lab = min(v, a);
+            got += claim(r, x, v, lab, CLS_TRIM2);
+            got += claim(r, x, a, lab, CLS_TRIM2);
+            break;
+        }
+    }
+    int64_t t = block_sum64(got, sh);
+    if (threadIdx.x == 0 && t) atomicAdd(r.counters + C_TRIM2, (unsigned long long)t);
+}
+
+// trim_3_1_from_fq (src/trim_2_3.h:482-677, cycle A->B->C->A) and
+// trim_3_2_from_fq (:881-1080, hub A<->B, A<->C) in one launch: both claim
+// 3-vertex sets, so they may run concurrently.  Label = min of the three.
+template <typename OffT>
+__global__ void __launch_bounds__(kBlock) k_trim3(Run<OffT> r, Ext<OffT> x, int in) {
+    __shared__ int64_t sh[kWarps];
+    const int64_t n = (int64_t)__ldcg(x.ctl + K_WL0 + in);
+    const int32_t *wl = r.wl[in];
+    int64_t got = 0;
+    for (int64_t i = (int64_t)blockIdx.x * kBlock + threadIdx.x; i < n; i += (int64_t)gridDim.x * kBlock) {
+        int32_t v = wl[i];
+        if (!bitv(r.A, v)) continue;
+        for (int dir = 0; dir < 2; ++dir) {
+            const OffT *beg = dir == 0 ? r.fw_beg : r.bw_beg;
+            const int32_t *adj = dir == 0 ? r.fw_adj : r.bw_adj;
+            int32_t B = -1, C = -1, y = -1, z = -1;
+            int nv = distinct_active(beg, adj, r.A, v, v, v, 3, B, C);
+            int32_t m0 = -1, m1 = -1, m2 = -1;
+            if (nv == 1) {  // cycle shape: v -> B -> C -> v
+                if (distinct_active(beg, adj, r.A, B, B, v, 2, y, z) != 1) continue;
+                int32_t Cc = y;
+                if (distinct_active(beg, adj, r.A, Cc, Cc, B, 2, y, z) != 1 || y != v) continue;
+                m0 = v; m1 = B; m2 = Cc;
+            } else if (nv == 2) {  // hub shape: v <-> B, v <-> C
+                if (distinct_active(beg, adj, r.A, B, B, C, 2, y, z) != 1 || y != v) continue;
+                if (distinct_active(beg, adj, r.A, C, C, B, 2, y, z) != 1 || y != v) continue;
+                m0 = v; m1 = B; m2 = C;
+            } else {
+                continue;
+            }
+            int32_t lab = min(m0, min(m1, m2));
+            got += claim(r, x, m0, lab, CLS_TRIM3);
+            got += claim(r, x, m1, lab, CLS_TRIM3);
+            got += claim(r, x, m2, lab, CLS_TRIM3);
+            break;
+        }
+    }
+    int64_t t = block_sum64(got, sh);
+    if (threadIdx.x == 0 && t) atomicAdd(r.counters + C_TRIM3, (unsigned long long)t);
+}
+
+// ---------------------------------------------------------------------------
+// Weakly connected components of the residual: hook-and-pointer-jump
+// union-find (replaces coloring_wcc, src/color_propagation.h:468-593, and the
+// unused openmp_wcc, src/openmp_wcc.hpp:14-165).  Roots are hooked under the
+// smaller id, so every root is its component's minimum vertex and parent ids
+// strictly decrease along a path; path halving keeps that invariant.
+__device__ __forceinline__ int32_t uf_find(int32_t *parent, int32_t x) {
+    int32_t p = __ldcg(parent + x);
+    while (p != x) {
+        int32_t gp = __ldcg(parent + p);
+        if (gp != p) parent[x] = gp;  // halving; gp < p < x
+        x = p;
+        p = gp;
+    }
+    return x;
+}
+
+template <typename OffT>
+__global__ void __launch_bounds__(kBlock) k_wcc_init(Run<OffT> r, Ext<OffT> x, int in) {
+    const int64_t n = (int64_t)__ldcg(x.ctl + K_WL0 + in);
+    for (int64_t i = (int64_t)blockIdx.x * kBlock + threadIdx.x; i < n; i += (int64_t)gridDim.x * kBlock) {
+        int32_t v = r.wl[in][i];
+        r.parent[v] = v;
+        r.aux[v] = 0;      // member count (valid at roots)
+        r.aux2[v] = -1;    // member base of a small WCC
+        r.cnt_out[v] = 0;  // fill cursor
+    }
+}
+
+template <typename OffT>
+__global__ void __launch_bounds__(kBlock) k_wcc_hook(Run<OffT> r, Ext<OffT> x, int in) {
+    const int64_t n = (int64_t)__ldcg(x.ctl + K_WL0 + in);
+    for (int64_t i = (int64_t)blockIdx.x * kBlock + threadIdx.x; i < n; i += (int64_t)gridDim.x * kBlock) {
+        int32_t v = r.wl[in][i];
+        int64_t e0 = ld_off(r.fw_beg, v), e1 = ld_off(r.fw_beg, v + 1);
+        for (int64_t e = e0; e < e1; ++e) {
+            int32_t w = __ldg(r.fw_adj + e);
+            if (w == v || !bitc(r.A, w)) continue;
+            int32_t a = v, b = w;
+            for (int guard = 0; guard < (1 << 20); ++guard) {
+                a = uf_find(r.parent, a);
+                b = uf_find(r.parent, b);
+                if (a == b) break;
+                if (a > b) { int32_t t = a; a = b; b = t; }
+                int32_t old = atomicCAS(r.parent + b, b, a);  // hook root b under a
+                if (old == b) break;
+                b = old;
+            }
+        }
+    }
+}
+
+// flatten, count members per root, list the roots
+template <typename OffT>
+__global__ void __launch_bounds__(kBlock) k_wcc_flatten(Run<OffT> r, Ext<OffT> x, int in) {
+    const int64_t n = (int64_t)__ldcg(x.ctl + K_WL0 + in);
+    for (int64_t i = (int64_t)blockIdx.x * kBlock + threadIdx.x; i - threadIdx.x < n;
+         i += (int64_t)gridDim.x * kBlock) {
+        bool isroot = false;
+        int32_t v = 0;
+        if (i < n) {
+            v = r.wl[in][i];
+            int32_t root = uf_find(r.parent, v);
+            r.parent[v] = root;
+            isroot = root == v;
+            // warp-aggregate the member count per distinct root
+            unsigned grp = __match_any_sync(__activemask(), root);
+            if (lane_id() == __ffs(grp) - 1) atomicAdd(r.aux + root, __popc(grp));
+        }
+        wl_append(isroot, v, x.roots, x.ctl + K_ROOTS);
+    }
+}
+
+// Reserve member space for small WCCs; route the rest to the large path.
+template <typename OffT>
+__global__ void __launch_bounds__(kBlock) k_wcc_alloc(Run<OffT> r, Ext<OffT> x) {
+    const int64_t n = (int64_t)__ldcg(x.ctl + K_ROOTS);
+    for (int64_t i = (int64_t)blockIdx.x * kBlock + threadIdx.x; i - threadIdx.x < n;
+         i += (int64_t)gridDim.x * kBlock) {
+        bool sm = false;
+        int32_t v = 0;
+        if (i < n) {
+            v = x.roots[i];
+            int32_t c = r.aux[v];
+            if (c <= kLocalV) {
+                r.aux2[v] = (int32_t)atomicAdd(x.ctl + K_ALLOC, (unsigned long long)c);
+                sm = true;
+            }
+        }
+        wl_append(sm, v, x.small, x.ctl + K_SMALL);
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(r.counters + C_WCC, (unsigned long long)n);
+}
+
+template <typename OffT>
+__global__ void __launch_bounds__(kBlock) k_wcc_scatter(Run<OffT> r, Ext<OffT> x, int in) {
+    const int64_t n = (int64_t)__ldcg(x.ctl + K_WL0 + in);
+    for (int64_t i = (int64_t)blockIdx.x * kBlock + threadIdx.x; i - threadIdx.x < n;
+         i += (int64_t)gridDim.x * kBlock) {
+        bool big = false;
+        int32_t v = 0;
+        if (i < n) {
+            v = r.wl[in][i];
+            int32_t root = r.parent[v];
+            int32_t b = r.aux2[root];
+            if (b >= 0) {
+                int32_t k = atomicAdd(r.cnt_out + root, 1);
+                r.members[b + k] = v;
+                r.cnt_in[v] = k;  // local index inside the WCC
+            } else {
+                big = true;
+            }
+        }
+        wl_append(big, v, x.large[0], x.ctl + K_LARGE);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Small WCCs: one CTA per WCC builds the induced subgraph in shared memory
+// and runs an iterative Tarjan on it (linear time; the reference's
+// mice_fw_bw, src/fw_bw.h:1585-1691, runs one forward-backward search per
+// pivot instead).  A WCC whose internal edges exceed kLocalE spills to the
+// large (colouring) path.
+constexpr int kLocalThreads = 256;
+
+template <typename OffT>
+__global__ void __launch_bounds__(kLocalThreads) k_local_scc(Run<OffT> r, Ext<OffT> x) {
+    __shared__ int32_t gid[kLocalV];
+    __shared__ int32_t loff[kLocalV + 1];
+    __shared__ uint16_t ladj[kLocalE];
+    __shared__ int16_t idx[kLocalV], low[kLocalV], stk[kLocalV], csv[kLocalV];
+    __shared__ int32_t cse[kLocalV];
+    __shared__ uint8_t onst[kLocalV];
+    const int64_t nsmall = (int64_t)__ldcg(x.ctl + K_SMALL);
+    for (int64_t wq = blockIdx.x; wq < nsmall; wq += gridDim.x) {
+        const int32_t root = x.small[wq];
+        const int32_t nv = r.aux[root];
+        const int32_t base = r.aux2[root];
+        // per-vertex internal out-degree, then a vertex-order scan by warp 0
+        for (int i = threadIdx.x; i < nv; i += kLocalThreads) {
+            int32_t u = r.members[base + i];
+            gid[i] = u;
+            int32_t dcount = 0;
+            int64_t e0 = ld_off(r.fw_beg, u), e1 = ld_off(r.fw_beg, u + 1);
+            for (int64_t e = e0; e < e1; ++e) {
+                int32_t w = __ldg(r.fw_adj + e);
+                dcount += (w != u) && bitc(r.A, w);
+            }
+            loff[i + 1] = dcount;
+        }
+        __syncthreads();
+        if (threadIdx.x < 32) {
+            int32_t carry = 0;
+            if (threadIdx.x == 0) loff[0] = 0;
+            for (int b0 = 0; b0 < nv; b0 += 32) {
+                int i = b0 + threadIdx.x;
+                int32_t inc = i < nv ? loff[i + 1] : 0;
+                for (int o = 1; o < 32; o <<= 1) {
+                    int32_t y = __shfl_up_sync(kFull, inc, o);
+                    if (lane_id() >= o) inc += y;
+                }
+                if (i < nv) loff[i + 1] = carry + inc;
+                carry += __shfl_sync(kFull, inc, 31);
+            }
+        }
+        __syncthreads();
+        const int32_t tot = loff[nv];
+        if (tot > kLocalE) {
+            // spill: hand the whole WCC to the colouring path
+            for (int i = threadIdx.x; i < nv; i += kLocalThreads) {
+                unsigned long long p = atomicAdd(x.ctl + K_LARGE, 1ull);
+                x.large[0][p] = gid[i];
+            }
+            if (threadIdx.x == 0) atomicAdd(r.counters + C_SPILL, 1ull);
+            __syncthreads();
+            continue;
+        }
+        // fill local adjacency (local ids from the scatter pass)
+        for (int i = threadIdx.x; i < nv; i += kLocalThreads) {
+            {
+                int32_t u = gid[i];
+                int32_t p = loff[i];
+                int64_t e0 = ld_off(r.fw_beg, u), e1 = ld_off(r.fw_beg, u + 1);
+                for (int64_t e = e0; e < e1; ++e) {
+                    int32_t w = __ldg(r.fw_adj + e);
+                    if (w != u && bitc(r.A, w)) ladj[p++] = (uint16_t)r.cnt_in[w];
+                }
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            // iterative Tarjan over the local CSR
+            for (int i = 0; i < nv; ++i) { idx[i] = -1; onst[i] = 0; }
+            int counter = 0, sp = 0, nscc = 0;
+            for (int s0 = 0; s0 < nv; ++s0) {
+                if (idx[s0] != -1) continue;
+                int cp = 0;
+                csv[0] = (int16_t)s0; cse[0] = loff[s0]; cp = 1;
+                idx[s0] = low[s0] = (int16_t)counter++;
+                stk[sp++] = (int16_t)s0; onst[s0] = 1;
+                while (cp > 0) {
+                    int vv = csv[cp - 1];
+                    int e = cse[cp - 1];
+                    bool down = false;
+                    for (; e < loff[vv + 1]; ++e) {
+                        int w = ladj[e];
+                        if (idx[w] == -1) {
+                            cse[cp - 1] = e + 1;
+                            idx[w] = low[w] = (int16_t)counter++;
+                            stk[sp++] = (int16_t)w; onst[w] = 1;
+                            csv[cp] = (int16_t)w; cse[cp] = loff[w]; cp++;
+                            down = true;
+                            break;
+                        } else if (onst[w] && idx[w] < low[vv]) {
+                            low[vv] = idx[w];
+                        }
+                    }
+                    if (down) continue;
+                    if (low[vv] == idx[vv]) {
+                        int32_t mn = 0x7fffffff, k = sp, sz = 0;
+                        do { --k; mn = min(mn, gid[stk[k]]); ++sz; } while (stk[k] != vv);
+                        while (sp > k) {
+                            int w = stk[--sp];
+                            onst[w] = 0;
+                            r.label[gid[w]] = mn;
+                            r.cls[gid[w]] = CLS_MICE;
+                        }
+                        atomicAdd((unsigned long long *)(r.hist + sz), 1ull);  // sz <= kLocalV
+                        ++nscc;
+                    }
+                    cp--;
+                    if (cp > 0) {
+                        int p = csv[cp - 1];
+                        if (low[vv] < low[p]) low[p] = low[vv];
+                    }
+                }
+            }
+            atomicAdd(r.counters + C_MICE_SCC, (unsigned long long)nscc);
+            atomicAdd(r.counters + C_MICE_V, (unsigned long long)nv);
+            atomicAdd(r.counters + C_LOCAL_WCC, 1ull);
+        }
+        __syncthreads();
+        // the WCC is done: leave the active map
+        for (int i = threadIdx.x; i < nv; i += kLocalThreads) clear_bit(r.A, gid[i]);
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Large WCCs: colouring rounds (the reference's dead color_propagation /
+// color_identify, src/color_propagation.h:64-466, restated as the pipeline's
+// mice stage).  Per round: every active vertex starts with its own id as
+// colour; colours relax to the minimum over all forward ancestors with a
+// frontier-driven propagation; a vertex whose colour is its own id is a root;
+// a backward search from all roots at once, restricted to the root's colour,
+// collects exactly the root's SCC (all ancestors of a member reach the root,
+// so the member's colour is the root's id; the root is the SCC's minimum
+// vertex, i.e. its canonical label).  Found SCCs leave; the rest recolour.
+template <typename OffT>
+__global__ void __launch_bounds__(kBlock) k_color(Run<OffT> r, Ext<OffT> x) {
+    __shared__ int64_t sh[kWarps];
+    const int64_t gt = (int64_t)blockIdx.x * kBlock + threadIdx.x;
+    const int64_t nt = (int64_t)gridDim.x * kBlock;
+    int32_t *col = r.parent;
+    unsigned long long *cqc = x.ctl + K_CQ0;
+    int cur = 0;
+    int rounds = 0;
+    for (int guard = 0; guard < (1 << 30); ++guard) {
+        const int64_t n = (int64_t)__ldcg(x.ctl + (cur == 0 ? K_LARGE : K_LARGE2));
+        if (n == 0) break;
+        ++rounds;
+        const int32_t *L = x.large[cur];
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            cqc[0] = 0; cqc[1] = 0; cqc[2] = 0;
+            x.ctl[cur == 0 ? K_LARGE2 : K_LARGE] = 0;
+        }
+        for (int64_t i = gt; i < n; i += nt) {
+            int32_t v = L[i];
+            col[v] = v;
+            r.aux[v] = 0;       // SCC size at roots
+            clear_bit(r.F, v);  // F: SCC mark of this round
+            clear_bit(r.D, v);  // D: queued-this-level mark
+        }
+        if (!grid_sync(r.gsync, r.err)) return;
+        // forward min-colour propagation: level 0 queue = L itself
+        int lv = 0;
+        for (int g2 = 0; g2 < (1 << 30); ++g2) {
+            const int64_t m = lv == 0 ? n : (int64_t)__ldcg(cqc + lv % 3);
+            if (m == 0) break;
+            if (blockIdx.x == 0 && threadIdx.x == 0) cqc[(lv + 2) % 3] = 0ull;
+            const int32_t *q = lv == 0 ? L : x.cq[lv & 1];
+            int32_t *qn = x.cq[(lv + 1) & 1];
+            for (int64_t i = gt; i - threadIdx.x < m; i += nt) {
+                bool live = i < m;
+                int32_t v = live ? __ldcg(q + i) : 0;
+                if (live && lv > 0) {
+                    clear_bit(r.D, v);
+                    __threadfence();  // clear the queued mark before reading the colour
+                }
+                int32_t c = live ? __ldcg(col + v) : 0;
+                int64_t e0 = live ? ld_off(r.fw_beg, v) : 0, e1 = live ? ld_off(r.fw_beg, v + 1) : 0;
+                int64_t len = e1 - e0, maxlen = len;
+                for (int o = 16; o; o >>= 1) maxlen = max(maxlen, __shfl_xor_sync(kFull, maxlen, o));
+                for (int64_t k = 0; k < maxlen; ++k) {
+                    bool push = false;
+                    int32_t w = 0;
+                    if (k < len) {
+                        w = __ldg(r.fw_adj + e0 + k);
+                        if (w != v && bitv(r.A, w) && c < __ldcg(col + w)) {
+                            int32_t old = atomicMin(col + w, c);
+                            if (c < old) {
+                                __threadfence();  // the new colour is visible before the mark test
+                                push = set_bit(r.D, w);
+                            }
+                        }
+                    }
+                    wl_append(push, w, qn, cqc + (lv + 1) % 3);
+                }
+            }
+            if (!grid_sync(r.gsync, r.err)) return;
+            ++lv;
+        }
+        // backward search from the roots inside each colour
+        if (blockIdx.x == 0 && threadIdx.x == 0) { cqc[0] = 0; cqc[1] = 0; cqc[2] = 0; }
+        if (!grid_sync(r.gsync, r.err)) return;
+        for (int64_t i = gt; i - threadIdx.x < n; i += nt) {
+            bool rt = false;
+            int32_t v = 0;
+            if (i < n) {
+                v = L[i];
+                rt = __ldcg(col + v) == v;
+                if (rt) set_bit(r.F, v);
+            }
+            wl_append(rt, v, x.cq[0], cqc + 0);
+        }
+        if (!grid_sync(r.gsync, r.err)) return;
+        lv = 0;
+        for (int g2 = 0; g2 < (1 << 30); ++g2) {
+            const int64_t m = (int64_t)__ldcg(cqc + lv % 3);
+            if (m == 0) break;
+            if (blockIdx.x == 0 && threadIdx.x == 0) cqc[(lv + 2) % 3] = 0ull;
+            const int32_t *q = x.cq[lv & 1];
+            int32_t *qn = x.cq[(lv + 1) & 1];
+            for (int64_t i = gt; i - threadIdx.x < m; i += nt) {
+                bool live = i < m;
+                int32_t v = live ? __ldcg(q + i) : 0;
+                int32_t c = live ? __ldcg(col + v) : 0;
+                int64_t e0 = live ? ld_off(r.bw_beg, v) : 0, e1 = live ? ld_off(r.bw_beg, v + 1) : 0;
+                int64_t len = e1 - e0, maxlen = len;
+                for (int o = 16; o; o >>= 1) maxlen = max(maxlen, __shfl_xor_sync(kFull, maxlen, o));
+                for (int64_t k = 0; k < maxlen; ++k) {
+                    bool push = false;
+                    int32_t u = 0;
+                    if (k < len) {
+                        u = __ldg(r.bw_adj + e0 + k);
+                        if (u != v && bitv(r.A, u) && __ldcg(col + u) == c && !bitv(r.F, u)) push = set_bit(r.F, u);
+                    }
+                    wl_append(push, u, qn, cqc + (lv + 1) % 3);
+                }
+            }
+            if (!grid_sync(r.gsync, r.err)) return;
+            ++lv;
+        }
+        // label the found SCCs, keep the rest for the next round
+        int64_t nl = 0;
+        for (int64_t i = gt; i - threadIdx.x < n; i += nt) {
+            bool keep = false;
+            int32_t v = 0;
+            if (i < n) {
+                v = L[i];
+                if (bitv(r.F, v)) {
+                    int32_t c = __ldcg(col + v);
+                    r.label[v] = c;
+                    r.cls[v] = CLS_MICE;
+                    atomicAdd(r.aux + c, 1);
+                    ++nl;
+                } else {
+                    keep = true;
+                }
+            }
+            wl_append(keep, v, x.large[cur ^ 1], x.ctl + (cur == 0 ? K_LARGE2 : K_LARGE));
+        }
+        if (!grid_sync(r.gsync, r.err)) return;
+        int64_t nroots = 0;
+        for (int64_t i = gt; i < n; i += nt) {
+            int32_t v = L[i];
+            if (bitv(r.F, v)) {
+                clear_bit(r.A, v);
+                if (__ldcg(col + v) == v) {
+                    int32_t sz = __ldcg(r.aux + v);
+                    if (sz < kHistCap) {
+                        atomicAdd((unsigned long long *)(r.hist + sz), 1ull);
+                    } else {
+                        unsigned long long k = atomicAdd(r.counters + C_BIG, 1ull);
+                        if (k < kBigCap) r.hist[kHistCap + k] = sz;
+                    }
+                    ++nroots;
+                }
+            }
+        }
+        int64_t a = block_sum64(nl, sh), b = block_sum64(nroots, sh);
+        if (threadIdx.x == 0) {
+            if (a) atomicAdd(r.counters + C_MICE_V, (unsigned long long)a);
+            if (b) atomicAdd(r.counters + C_MICE_SCC, (unsigned long long)b);
+        }
+        if (!grid_sync(r.gsync, r.err)) return;
+        cur ^= 1;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) r.counters[C_COLOR_ROUNDS] = (unsigned long long)rounds;
+}
+
+// ---------------------------------------------------------------------------
+// Final labels of the giant SCCs, histogram entries of the classes whose
+// sizes are fixed, and the per-graph giant sizes.  Any vertex still active
+// here is an internal error.
+template <typename OffT>
+__global__ void __launch_bounds__(kBlock) k_finalize(Run<OffT> r, Ext<OffT> x) {
+    const int lane = lane_id();
+    const int64_t gw = ((int64_t)blockIdx.x * kBlock + threadIdx.x) >> 5;
+    const int64_t nw = (int64_t)gridDim.x * kWarps;
+    for (int64_t wi = gw; wi < r.W; wi += nw) {
+        uint32_t s = r.B[wi];
+        if (r.A[wi] && lane == 0) atomicCAS(r.err, 0, kErrOverflow);
+        if (!s) continue;
+        int64_t v = wi * 32 + lane;
+        if ((s >> lane) & 1u) r.label[v] = r.gmin[seg_of(r.vbase, r.nseg, v)];
+    }
+    const int64_t gt = (int64_t)blockIdx.x * kBlock + threadIdx.x;
+    for (int64_t sg = gt; sg < r.nseg; sg += (int64_t)gridDim.x * kBlock) {
+        unsigned long long sz = r.gsize[sg];
+        if (!sz) continue;
+        atomicAdd(r.counters + C_GIANTS, 1ull);
+        if (sz < (unsigned long long)kHistCap) {
+            atomicAdd((unsigned long long *)(r.hist + sz), 1ull);
+        } else {
+            unsigned long long k = atomicAdd(r.counters + C_BIG, 1ull);
+            if (k < kBigCap) r.hist[kHistCap + k] = (int64_t)sz;
+        }
+    }
+    if (gt == 0) {
+        unsigned long long t1 = r.counters[C_TRIM1], t2 = r.counters[C_TRIM2], t3 = r.counters[C_TRIM3];
+        atomicAdd((unsigned long long *)(r.hist + 1), t1);
+        atomicAdd((unsigned long long *)(r.hist + 2), t2 / 2);
+        atomicAdd((unsigned long long *)(r.hist + 3), t3 / 3);
+    }
+}
+
+}  // namespace ispan
