@@ -1,0 +1,385 @@
+"""Benchmark of the B200 SCC pipeline on the social-network workload.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload social|rmat16|web|batch] [--scale S]
+
+Workload (default "social"): a seeded synthetic directed power-law graph with
+the sizes of the Twitter crawl the reference reports on (41,652,231 vertices,
+~1.47 B edges after dedupe, ~80 % of the vertices in one giant SCC, the rest
+in size-1/2/3 SCCs and a power-law tail of cycles), int32 ids and int64
+offsets, generated on the GPU.  One step = one full SCC detection over that
+graph (trim, FW/BW, peel, trim-2/3, WCC, mice, canonical labels).
+
+Metric: SCC GTEPS = E / t_step / 1e9 (the reference's convention: whole
+pipeline time, graph load excluded).  ``value`` is measured with the CSR
+resident in HBM; ``e2e`` through the public API with pinned host buffers,
+the H2D upload of the CSR and the D2H copy of the labels inside the timed
+region.  Multi-GPU: the single-graph pipeline does not shard; N ranks run N
+independent replicas (weak scaling, no collective on the data path).
+
+--impl reference runs the reference's own OpenMP pipeline (its unmodified
+CLI, compiled from its sources into oracle/_ref/) on the host cores, on the
+same graph written in its int32 binary format.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+REF_PARAMS = ("30", "200", "10", "0.1")  # src/bash_one.sh:4
+KERNELS_PER_STEP = 19  # stage kernels enqueued per pipeline run (pipeline.cu: enqueue)
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing (one process per GPU, torchrun)
+
+def dist_init():
+    import torch
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if torch.cuda.is_available():
+        torch.cuda.set_device(local)
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        dist.init_process_group("nccl" if torch.cuda.is_available() else "gloo",
+                                timeout=datetime.timedelta(seconds=300))
+    return ws, rank, local
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, ws):
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda" if torch.cuda.is_available() else "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+
+class Clocks:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.p = None
+        self.f = None
+
+    def start(self):
+        if not shutil.which("nvidia-smi"):
+            return
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.Q}",
+                                   "--format=csv,noheader,nounits", "-lms", "200"],
+                                  stdout=self.f, stderr=subprocess.DEVNULL)
+
+    def stop(self):
+        if not self.p:
+            return None
+        time.sleep(0.25)
+        self.p.terminate()
+        try:
+            self.p.wait(5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        rows = [r.split(",") for r in open(self.f.name).read().strip().splitlines() if r.count(",") >= 8]
+        os.unlink(self.f.name)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if "Active" in v and "Not" not in v})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------
+# workloads
+
+def make_graph(workload, seed, scale):
+    from ispan_b200 import gen
+    if workload == "social":
+        g = gen.social(seed=seed, scale=scale)
+        desc = {"workload": "social-network SCC (Twitter-sized synthetic power-law digraph)",
+                "vertices": g.V, "edges": g.E, "giant_frac_target": 0.80, "offsets": "int64",
+                "ids": "int32", "seed": seed, "scale": scale}
+    elif workload == "rmat16":
+        g = gen.rmat(16, 16, seed)
+        desc = {"workload": "R-MAT scale 16 edge factor 16 (a,b,c)=(.57,.19,.19)", "vertices": g.V,
+                "edges": g.E, "offsets": "int64", "ids": "int32", "seed": seed}
+    elif workload == "web":
+        g = gen.web(seed=seed, scale=scale)
+        desc = {"workload": "web-crawl SCC (giant 35%, trivial 50%, planted mid-size SCCs in a DAG)",
+                "vertices": g.V, "edges": g.E, "offsets": "int64", "ids": "int32", "seed": seed, "scale": scale}
+    else:
+        raise SystemExit(f"unknown workload {workload}")
+    return g, desc
+
+
+def alg_bytes(st, o=8, s=1):
+    """Algorithmic bytes of the FW and BW searches: 4 B per edge of the
+    reached set, two offsets and one status byte per reached vertex."""
+    fw = 4 * st["fw_edges"] + 2 * o * st["fw_size"] + s * st["fw_size"]
+    bw = 4 * st["bw_edges"] + 2 * o * st["giant_size"] + s * st["giant_size"]
+    return fw, bw
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        return float(json.load(open(p))["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def traffic_from_profiles(kernel):
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get(kernel)
+    return None
+
+
+# ---------------------------------------------------------------------------
+# the reference's own CLI on the host
+
+def host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def write_ref_files(g, d):
+    """The graph in the reference's binary format (int32 offsets and ids)."""
+    from ispan_b200.graphs import write_bin
+    csr = g.to_host(np.int32)
+    return write_bin(csr, d, np.int32), csr
+
+
+def run_reference_cli(paths, threads, runs, timeout):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    if not os.path.exists(oracle.REF_BIN):
+        raise FileNotFoundError("oracle/_ref/ispan not built (make -C oracle ref where the reference tree is)")
+    cmd = [oracle.REF_BIN, *paths, str(threads), *REF_PARAMS, str(runs)]
+    r = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout)
+    if r.returncode != 0:
+        raise RuntimeError(f"reference exited {r.returncode}: {r.stderr[-300:]}")
+    totals = [float(line.split(",")[1]) for line in r.stdout.splitlines() if line.startswith("total time,")]
+    if not totals:
+        raise RuntimeError("reference printed no per-run total time")
+    return totals, r.stdout
+
+
+def tmpdir_for(nbytes):
+    for base in ("/dev/shm", tempfile.gettempdir()):
+        try:
+            if shutil.disk_usage(base).free > nbytes * 1.2:
+                return tempfile.mkdtemp(dir=base, prefix="ispan_ref_")
+        except OSError:
+            pass
+    return tempfile.mkdtemp(prefix="ispan_ref_")
+
+
+def reference_timing(g, steps, warmup, timeout=900):
+    """Per-run totals (ms) of the reference's unmodified CLI on this graph."""
+    d = tmpdir_for(8 * g.E + 8 * g.V)
+    try:
+        paths, _ = write_ref_files(g, d)
+        totals, out = run_reference_cli(paths, host_threads(), warmup + steps, timeout)
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+    return totals[warmup:] if len(totals) > warmup else totals
+
+
+# ---------------------------------------------------------------------------
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="social")
+    ap.add_argument("--scale", type=float, default=1.0)
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-steps", type=int, default=2, help="reference runs for cpu_baseline")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        log("warmup raised to 3 (timing rule)")
+        args.warmup = 3
+
+    ws, rank, local = dist_init()
+    import torch
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        g, desc = make_graph(args.workload, args.seed, args.scale)
+        try:
+            totals = reference_timing(g, args.steps, args.warmup)
+        except (FileNotFoundError, RuntimeError, subprocess.TimeoutExpired) as e:
+            print(json.dumps({"impl": "reference", "unavailable": str(e).splitlines()[0][:300]}))
+            return
+        ms = statistics.mean(totals)
+        val = g.E / (ms / 1e3) / 1e9
+        th = host_threads()
+        print(json.dumps({
+            "impl": "reference", "metric": "SCC GTEPS", "value": val, "unit": "GTEPS", "n_gpus": ws,
+            "steps": len(totals), "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+            "config": dict(desc, parallelism=f"openmp{th}"),
+            "cpu_baseline": {"value": val, "unit": "GTEPS", "cores": th, "kind": "reference",
+                             "sample": f"full graph, {len(totals)} timed runs of the reference CLI "
+                                       f"(src/scc_main.cpp) after {args.warmup} warm-up runs"},
+            "e2e": {"value": val, "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+        return
+
+    from ispan_b200 import Context
+    g, desc = make_graph(args.workload, args.seed, args.scale)
+    log(f"[rank {rank}] graph V={g.V} E={g.E}")
+    stream = torch.cuda.Stream()
+    ctx = Context(g.V, g.E)
+    ctx.set_stream(stream)
+    fb, fa, bb, ba = g.to_torch("int64")
+    labels = torch.empty(g.V, dtype=torch.int32, device="cuda")
+    run = lambda: ctx.run(fb, fa, bb, ba, V=g.V, labels_out=labels, stage_times=True)  # noqa: E731
+    for _ in range(args.warmup):
+        _, st = run()
+    torch.cuda.synchronize()
+
+    # ---- timed region: K steps, inputs resident in HBM (12 GB > L2) ----
+    clocks = Clocks(local)
+    barrier(ws)
+    torch.cuda.synchronize()
+    clocks.start()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    stages = []
+    ev[0].record(stream)
+    for k in range(args.steps):
+        _, st = run()
+        ev[k + 1].record(stream)
+        stages.append(st)
+    torch.cuda.synchronize()
+    barrier(ws)
+    clk = clocks.stop()
+    step_ms = [ev[k].elapsed_time(ev[k + 1]) for k in range(args.steps)]
+    total_ms = ev[0].elapsed_time(ev[-1])
+    total_ms_max = max_over_ranks(total_ms, ws)
+    ms_per_step = total_ms_max / args.steps
+    value = ws * g.E / (ms_per_step / 1e3) / 1e9
+
+    # roofline of the dominant kernel (the longer of the FW and BW searches)
+    fw_b, bw_b = alg_bytes(st)
+    fw_ms = statistics.mean(s["stage_ms"][7] for s in stages)
+    bw_ms = statistics.mean(s["stage_ms"][8] for s in stages)
+    kern, by, kms = ("k_bfs<int64,0> (forward reach)", fw_b, fw_ms) if fw_ms >= bw_ms else \
+        ("k_bfs<int64,1> (backward reach)", bw_b, bw_ms)
+    peak, peak_kind = measured_peak()
+    achieved = by / (kms / 1e3) / 1e9
+    traffic = traffic_from_profiles("k_bfs_fw" if "0>" in kern else "k_bfs_bw")
+    roof = {"bound": "hbm", "kernel": kern, "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
+            "alg_bytes_per_launch": by, "kernel_ms": kms}
+    stage_mean = [statistics.mean(s["stage_ms"][i] for s in stages) for i in range(16)]
+
+    # ---- end to end through the public API with pinned host buffers ----
+    e2e = None
+    if args.e2e_steps > 0:
+        hfb = torch.empty(g.V + 1, dtype=torch.int64, pin_memory=True)
+        hbb = torch.empty(g.V + 1, dtype=torch.int64, pin_memory=True)
+        hfa = torch.empty(g.E, dtype=torch.int32, pin_memory=True)
+        hba = torch.empty(g.E, dtype=torch.int32, pin_memory=True)
+        hfb.copy_(fb)
+        hbb.copy_(bb)
+        hfa.copy_(fa)
+        hba.copy_(ba)
+        hlab = torch.empty(g.V, dtype=torch.int32, pin_memory=True)
+        np_args = [t.numpy() for t in (hfb, hfa, hbb, hba)]
+        del fb, fa, bb, ba
+        torch.cuda.empty_cache()
+        ctx.run(*np_args, V=g.V, labels_out=hlab.numpy())  # warm (allocates the upload buffers)
+        barrier(ws)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.e2e_steps):
+            ctx.run(*np_args, V=g.V, labels_out=hlab.numpy())
+        e1.record(stream)
+        torch.cuda.synchronize()
+        e2e_ms = max_over_ranks(e0.elapsed_time(e1), ws) / args.e2e_steps
+        h2d = 2 * (g.V + 1) * 8 + 2 * g.E * 4
+        e2e = {"value": ws * g.E / (e2e_ms / 1e3) / 1e9, "unit": "GTEPS", "ms_per_step": e2e_ms,
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": g.V * 4}
+
+    # ---- CPU baseline: the reference's own OpenMP build on this host ----
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        try:
+            totals = reference_timing(g, args.ref_steps, 1, timeout=600)
+            cms = statistics.mean(totals)
+            cpu = {"value": g.E / (cms / 1e3) / 1e9, "unit": "GTEPS", "cores": host_threads(),
+                   "kind": "reference", "ms_per_run": cms,
+                   "sample": f"the full graph, {len(totals)} runs of the reference CLI after 1 warm-up run"}
+        except Exception as e:  # noqa: BLE001
+            cpu = {"value": None, "unit": "GTEPS", "cores": host_threads(), "kind": "reference",
+                   "sample": f"unavailable: {str(e).splitlines()[0][:200]}"}
+
+    if rank == 0:
+        out = {
+            "metric": "SCC GTEPS", "value": value, "unit": "GTEPS", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+            "config": dict(desc, parallelism="replicas" if ws > 1 else "single-gpu",
+                           l2="inputs larger than L2 (CSR resident in HBM)"),
+            "e2e": e2e, "gpu_launches": KERNELS_PER_STEP * args.steps, "roofline": roof, "cpu_baseline": cpu,
+            "clocks": clk,
+            "stage_ms": {"trim": stage_mean[0], "elephant": stage_mean[1], "mice": stage_mean[2],
+                         "total": stage_mean[3], "fw": stage_mean[7], "bw": stage_mean[8], "wcc": stage_mean[9],
+                         "mice_scc": stage_mean[10], "trim2": stage_mean[5], "trim3": stage_mean[13]},
+            "scc": {k: st[k] for k in ("scc_count", "giant_size", "n_trim1", "n_trim2", "n_trim3",
+                                       "n_mice_scc", "fw_size", "fw_levels", "bw_levels", "color_rounds")},
+            "step_ms_min": min(step_ms), "step_ms_max": max(step_ms),
+        }
+        print(json.dumps(out))
+    ctx.close()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

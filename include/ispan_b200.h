@@ -63,6 +63,8 @@ typedef struct {
 #define ISPAN_F_NO_GRAPH 2u         /* launch stages directly, no CUDA graph */
 #define ISPAN_F_STAGE_TIMES 4u      /* record per-stage device times */
 #define ISPAN_F_NO_L2_WINDOW 8u     /* do not pin the status maps in L2 */
+#define ISPAN_F_VALIDATE 16u        /* check a device-resident CSR before the run
+                                       (host CSRs are always checked) */
 
 /* Stage-time slots follow the reference's avg_time[15] meanings
  * (src/scc_core.cpp:24-25, :1037-1053): 0 trim, 1 elephant SCC, 2 mice SCC,
@@ -75,6 +77,8 @@ typedef struct {
     int64_t n_trim1, n_trim2, n_trim3; /* vertices labelled by each trim */
     int64_t n_mice_vertices, n_mice_scc, n_wcc;
     int64_t fw_size, fw_levels, bw_levels, residual, color_rounds, local_wcc, trim_rounds;
+    int64_t fw_edges;         /* sum of out-degrees over the forward set F */
+    int64_t bw_edges;         /* sum of in-degrees over the pivot SCC(s) S */
     /* sparse size histogram: pairs (hist_size[i], hist_count[i]) sorted by
      * size; the caller supplies the arrays (hist_cap entries) or NULLs */
     int64_t *hist_size, *hist_count;

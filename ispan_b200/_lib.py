@@ -9,7 +9,9 @@ import ctypes as C
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libispan_b200.so")
+# ISPAN_CHECKED=1 loads the self-checking build (range checks on every index)
+LIB_PATH = os.path.join(HERE, "libispan_b200_checked.so" if os.environ.get("ISPAN_CHECKED") == "1"
+                        else "libispan_b200.so")
 
 ISPAN_OK = 0
 ERRORS = {-1: "ISPAN_ERR_ARG", -2: "ISPAN_ERR_NOMEM", -3: "ISPAN_ERR_CUDA", -4: "ISPAN_ERR_TIMEOUT",
@@ -19,6 +21,7 @@ F_LABELS_ON_DEVICE = 1
 F_NO_GRAPH = 2
 F_STAGE_TIMES = 4
 F_NO_L2_WINDOW = 8
+F_VALIDATE = 16
 
 
 class IspanError(RuntimeError):
@@ -43,7 +46,8 @@ class Params(C.Structure):
 class Stats(C.Structure):
     _fields_ = [("stage_ms", C.c_double * 16)] + [(n, C.c_int64) for n in (
         "scc_count", "giant_size", "n_trim1", "n_trim2", "n_trim3", "n_mice_vertices", "n_mice_scc", "n_wcc",
-        "fw_size", "fw_levels", "bw_levels", "residual", "color_rounds", "local_wcc", "trim_rounds")] + [
+        "fw_size", "fw_levels", "bw_levels", "residual", "color_rounds", "local_wcc", "trim_rounds",
+        "fw_edges", "bw_edges")] + [
         ("hist_size", C.c_void_p), ("hist_count", C.c_void_p), ("hist_cap", C.c_int64), ("hist_n", C.c_int64)]
 
     def as_dict(self) -> dict:

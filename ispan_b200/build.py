@@ -21,9 +21,12 @@ FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--extended-lambda", "-Xcompiler", "-
          "-shared", "-I" + os.path.join(ROOT, "include")]
 
 TARGETS = {
-    "libispan_b200.so": (["pipeline.cu"], ["common.cuh", "bfs.cuh", "stages.cuh"]),
-    "libispan_gen.so": (["gen.cu"], []),
+    "libispan_b200.so": (["pipeline.cu"], ["common.cuh", "bfs.cuh", "stages.cuh"], []),
+    "libispan_gen.so": (["gen.cu"], [], []),
 }
+# self-checking variant: range checks on every index, first violation reported
+CHECKED = {"libispan_b200_checked.so": (["pipeline.cu"], ["common.cuh", "bfs.cuh", "stages.cuh"],
+                                        ["-DISPAN_CHECKED"])}
 
 
 def _stale(out, srcs):
@@ -34,15 +37,18 @@ def _stale(out, srcs):
     return any(os.path.getmtime(s) > t for s in deps if os.path.exists(s))
 
 
-def build(force: bool = False, verbose: bool = False, extra=()) -> list[str]:
+def build(force: bool = False, verbose: bool = False, extra=(), checked: bool = False) -> list[str]:
     outs = []
-    for lib, (srcs, hdrs) in TARGETS.items():
+    targets = dict(TARGETS)
+    if checked:
+        targets.update(CHECKED)
+    for lib, (srcs, hdrs, defs) in targets.items():
         src = [os.path.join(CSRC, s) for s in srcs]
         if not all(os.path.exists(s) for s in src):
             continue
         out = os.path.join(HERE, lib)
         if force or _stale(out, src + [os.path.join(CSRC, h) for h in hdrs]):
-            cmd = [NVCC, *ARCH, *FLAGS, *extra, *src, "-o", out]
+            cmd = [NVCC, *ARCH, *FLAGS, *defs, *extra, *src, "-o", out]
             if verbose:
                 print(" ".join(cmd), flush=True)
             subprocess.run(cmd, check=True)
@@ -51,5 +57,5 @@ def build(force: bool = False, verbose: bool = False, extra=()) -> list[str]:
 
 
 if __name__ == "__main__":
-    print("\n".join(build(force="--force" in sys.argv, verbose=True,
+    print("\n".join(build(force="--force" in sys.argv, verbose=True, checked="--checked" in sys.argv,
                           extra=["-Xptxas", "-v"] if "--ptxas" in sys.argv else [])))

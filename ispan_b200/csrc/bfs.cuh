@@ -82,6 +82,7 @@ __device__ __forceinline__ void td_chunk(const Run<OffT> &r, const BfsDir<OffT, 
     int64_t e1 = min(e0 + (int64_t)kChunk, qedges);
     int64_t s_lo = __ldcg(qc + c);
     int64_t s_hi = (c + 1 < nchunks) ? (int64_t)__ldcg(qc + c + 1) : qcount - 1;
+    if (!ICHK(s_lo >= 0 && s_lo <= s_hi && s_hi < qcount, 20, (s_lo << 32) | (s_hi & 0xffffffff))) return;
     // each thread owns a run of consecutive virtual edges, so one binary
     // search per thread finds its first slot and the walk follows the queue
     constexpr int kPer = kChunk / kBlock;
@@ -105,12 +106,13 @@ __device__ __forceinline__ void td_chunk(const Run<OffT> &r, const BfsDir<OffT, 
         int32_t w = -1;
         if (live) {
             while (e >= slot_e1) {  // advance to the slot that owns e
+                if (!ICHK(slot + 1 < qcount, 21, slot)) break;
                 ++slot;
                 slot_e0 = slot_e1;
                 slot_e1 = (slot + 1 < qcount) ? __ldcg(qe + slot + 1) : qedges;
                 base = ld_off(d.xbeg, __ldcg(qv + slot));
             }
-            w = __ldg(d.xadj + base + (e - slot_e0));
+            w = ld_adj(d.xadj, base + (e - slot_e0));
         }
         bool nw = false;
         if (live && bit(d.R, w) && !bitv(d.Vm, w)) nw = set_bit(d.Vm, w);
@@ -144,7 +146,7 @@ __device__ __forceinline__ void bu_words(const Run<OffT> &r, const BfsDir<OffT, 
             end = ld_off(d.pbeg, v + 1);
             int64_t cap = min(end, e + (int64_t)kBuLane);
             for (; e < cap; ++e)
-                if (bitv(d.Vm, __ldg(d.padj + e))) { found = true; break; }
+                if (bitv(d.Vm, ld_adj(d.padj, e))) { found = true; break; }
             rem = !found && e < end;
         }
         unsigned rm = __ballot_sync(kFull, rem);
@@ -155,7 +157,7 @@ __device__ __forceinline__ void bu_words(const Run<OffT> &r, const BfsDir<OffT, 
             bool hit = false;
             for (int64_t b = le; b < lend; b += 32) {
                 int64_t i = b + lane;
-                bool h = i < lend && bitv(d.Vm, __ldg(d.padj + i));
+                bool h = i < lend && bitv(d.Vm, ld_adj(d.padj, i));
                 if (__any_sync(kFull, h)) { hit = true; break; }
             }
             if (lane == l) found = hit;
@@ -221,7 +223,7 @@ __global__ void __launch_bounds__(kBlock) k_bfs(Run<OffT> r, BfsCtl *ctl) {
             if (blockIdx.x == 0) {
                 // CTA 0 alone: levels separated by __syncthreads only
                 int lv = level, exit_mode = M_DONE;
-                int64_t tv_all = 0, tm_all = 0;
+                int64_t tv_all = 0, tm_all = 0, tx_all = 0;
                 for (int it = 0; it < kTailMaxLevels; ++it) {
                     const int c2 = lv & 1;
                     const int sc = lv % 3, sn = (lv + 1) % 3, sf = (lv + 2) % 3;
@@ -233,8 +235,9 @@ __global__ void __launch_bounds__(kBlock) k_bfs(Run<OffT> r, BfsCtl *ctl) {
                     int64_t nch = (qe2 + kChunk - 1) / kChunk;
                     for (int64_t c = 0; c < nch; ++c)
                         td_chunk<OffT, DIR>(r, d, c, nch, qc2, qe2, c2, r.qpk + sn, nv, m1, m2, tid);
-                    tv_all += block_sum64(nv, sh);
+                        tv_all += block_sum64(nv, sh);
                     tm_all += block_sum64(m2, sh);
+                    tx_all += block_sum64(m1, sh);
                     ++lv;
                     unsigned long long pn = __ldcg(r.qpk + sn);
                     int64_t qcn = (int64_t)(pn & kCountMask), qen = (int64_t)(pn >> kCountBits);
@@ -245,6 +248,7 @@ __global__ void __launch_bounds__(kBlock) k_bfs(Run<OffT> r, BfsCtl *ctl) {
                 if (tid == 0) {
                     total_vis += tv_all;
                     if (DIR == 0 && tm_all) atomicAdd(r.counters + C_FW_MU, (unsigned long long)tm_all);
+                    if (tx_all) atomicAdd(r.counters + (DIR == 0 ? C_FW_XDEG : C_BW_XDEG), (unsigned long long)tx_all);
                     for (int i = 0; i < 3; ++i) slots[i] = LvlSlot{0, 0, 0, 0};
                     ctl->level = lv;
                     ctl->mode = exit_mode;
@@ -279,6 +283,8 @@ __global__ void __launch_bounds__(kBlock) k_bfs(Run<OffT> r, BfsCtl *ctl) {
         total_vis += nf;
         if (DIR == 0 && blockIdx.x == 0 && tid == 0 && s.m_other)
             atomicAdd(r.counters + C_FW_MU, s.m_other);
+        if (blockIdx.x == 0 && tid == 0 && s.m_next)
+            atomicAdd(r.counters + (DIR == 0 ? C_FW_XDEG : C_BW_XDEG), s.m_next);
         ++level;
         if (nf == 0) { mode = M_DONE; break; }
         m_unexpl -= (int64_t)s.m_next;

@@ -88,6 +88,8 @@ enum Counter {
     C_TRIM_ROUNDS,
     C_GIANTS,        // graphs whose pivot SCC is non-empty
     C_SPILL,         // small WCCs whose edges overflowed shared memory
+    C_FW_XDEG,       // sum of out-degrees over F  (algorithmic bytes of the FW search)
+    C_BW_XDEG,       // sum of in-degrees over S   (algorithmic bytes of the BW search)
     kNumCounters = 32
 };
 constexpr int kHistCap = 1 << 16;   // exact histogram for SCC sizes below this
@@ -98,25 +100,69 @@ constexpr int kErrTimeout = ISPAN_ERR_TIMEOUT;
 constexpr int kErrOverflow = ISPAN_ERR_INTERNAL;
 
 // ---------------------------------------------------------------------------
+// Self-checking build (-DISPAN_CHECKED): every vertex id, offset index,
+// adjacency position and queue slot is range-checked against the run's sizes;
+// the first violation is recorded (site, index) and the access is skipped, so
+// a bad index reports instead of faulting.  The normal build compiles the
+// checks away.
+#ifdef ISPAN_CHECKED
+__device__ long long g_vcap, g_ecap, g_qcap;  // V, E, chunk-table entries
+__device__ long long g_chk[2];                // first violation: site, index
+__device__ __noinline__ void chk_fail(int site, long long idx) {
+    if (atomicCAS((unsigned long long *)&g_chk[0], 0ull, (unsigned long long)site) == 0ull) g_chk[1] = idx;
+}
+#define ICHK(cond, site, idx) (__builtin_expect(!!(cond), 1) ? true : (chk_fail((site), (long long)(idx)), false))
+#else
+#define ICHK(cond, site, idx) true
+#endif
+#ifdef ISPAN_CHECKED
+#define VOK(v, site) ICHK((v) >= 0 && (v) < g_vcap + 32, site, v)
+#else
+#define VOK(v, site) true
+#endif
+
+#ifdef ISPAN_CHECKED
+__device__ __forceinline__ long long g_qcap_or(long long) { return g_qcap; }
+#else
+__device__ __forceinline__ long long g_qcap_or(long long x) { return x; }
+#endif
+
+// ---------------------------------------------------------------------------
 // small helpers
 __device__ __forceinline__ bool bit(const uint32_t *m, int64_t v) {
+    if (!VOK(v, 1)) return false;
     return (__ldg(m + (v >> 5)) >> (v & 31)) & 1u;
 }
 // coherent bit read (L2, not L1 or the read-only path): for maps that other
 // CTAs change while this kernel runs
 __device__ __forceinline__ bool bitv(const uint32_t *m, int64_t v) {
+    if (!VOK(v, 2)) return false;
     return (__ldcg(m + (v >> 5)) >> (v & 31)) & 1u;
 }
 __device__ __forceinline__ bool bitc(const uint32_t *m, int64_t v) {
+    if (!VOK(v, 3)) return false;
     return (m[v >> 5] >> (v & 31)) & 1u;
 }
 // set a bit; returns true if this call changed it from 0 to 1
 __device__ __forceinline__ bool set_bit(uint32_t *m, int64_t v) {
+    if (!VOK(v, 4)) return false;
     uint32_t b = 1u << (v & 31);
     return !(atomicOr(m + (v >> 5), b) & b);
 }
 __device__ __forceinline__ void clear_bit(uint32_t *m, int64_t v) {
+    if (!VOK(v, 5)) return;
     atomicAnd(m + (v >> 5), ~(1u << (v & 31)));
+}
+// adjacency entry e (a vertex id)
+__device__ __forceinline__ int32_t ld_adj(const int32_t *adj, int64_t e) {
+#ifdef ISPAN_CHECKED
+    if (!ICHK(e >= 0 && e < g_ecap, 6, e)) return 0;
+    int32_t w = __ldg(adj + e);
+    if (!ICHK(w >= 0 && w < g_vcap, 7, w)) return 0;
+    return w;
+#else
+    return __ldg(adj + e);
+#endif
 }
 __device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
 __device__ __forceinline__ unsigned lanemask_lt() {
@@ -130,7 +176,16 @@ __device__ __forceinline__ uint64_t globaltimer() {
     return t;
 }
 template <typename OffT>
-__device__ __forceinline__ int64_t ld_off(const OffT *p, int64_t i) { return (int64_t)__ldg(p + i); }
+__device__ __forceinline__ int64_t ld_off(const OffT *p, int64_t i) {
+#ifdef ISPAN_CHECKED
+    if (!ICHK(i >= 0 && i <= g_vcap, 8, i)) return 0;
+    int64_t x = (int64_t)__ldg(p + i);
+    if (!ICHK(x >= 0 && x <= g_ecap, 9, x)) return 0;
+    return x;
+#else
+    return (int64_t)__ldg(p + i);
+#endif
+}
 
 __device__ __forceinline__ int64_t warp_sum64(int64_t x) {
 #pragma unroll
@@ -246,16 +301,17 @@ __device__ __forceinline__ void q_append(bool pred, int32_t v, int64_t deg, int3
     if (me) {
         int64_t slot = (int64_t)(base & kCountMask) + __popc(m & lanemask_lt());
         int64_t eb = (int64_t)(base >> kCountBits) + incl - d;
-        if (slot < cap_v) {
+        if (ICHK(slot < cap_v, 10, slot)) {
             qv[slot] = v;
             qe[slot] = eb;
             int64_t c0 = (eb + kChunk - 1) / kChunk, c1 = (eb + d - 1) / kChunk;
-            for (int64_t c = c0; c <= c1; ++c) qchunk[c] = (int32_t)slot;
+            for (int64_t c = c0; c <= c1; ++c)
+                if (ICHK(c >= 0 && c < g_qcap_or(c + 1), 11, c)) qchunk[c] = (int32_t)slot;
         }
     }
 }
 
-// Warp-aggregated append of a vertex id to a plain worklist.
+// Warp-aggregated append of a vertex id to a plain worklist (capacity: V).
 __device__ __forceinline__ void wl_append(bool pred, int32_t v, int32_t *wl, unsigned long long *cnt) {
     unsigned m = __ballot_sync(kFull, pred);
     if (!m) return;
@@ -263,7 +319,10 @@ __device__ __forceinline__ void wl_append(bool pred, int32_t v, int32_t *wl, uns
     unsigned long long base = 0;
     if (lane_id() == leader) base = atomicAdd(cnt, (unsigned long long)__popc(m));
     base = __shfl_sync(kFull, base, leader);
-    if (pred) wl[base + __popc(m & lanemask_lt())] = v;
+    if (pred) {
+        unsigned long long at = base + __popc(m & lanemask_lt());
+        if (VOK((long long)at, 12)) wl[at] = v;
+    }
 }
 
 // segment of a vertex in a disjoint union (binary search over vbase)

@@ -110,6 +110,8 @@ struct ispan_ctx {
     int64_t last_V = 0;
     int32_t *last_label = nullptr;
     int64_t last_nseg = 1;
+    std::vector<int64_t> vbase_host;  // segmentation currently on the device
+    bool validate_next = false;       // an uploaded host CSR is checked once on the device
     std::mutex mu;
 };
 
@@ -189,6 +191,7 @@ static int ctx_segments(ispan_ctx *c, int64_t nseg) {
         cudaGraphExecDestroy(c->gexec);
         c->gexec = nullptr;
     }
+    c->vbase_host.clear();
     return ISPAN_OK;
 }
 
@@ -261,13 +264,13 @@ static cudaError_t launch_coop(Kern k, int grid, cudaStream_t s, Args... args) {
 
 // Enqueue the whole pipeline on c->stream (plain launches; may be captured).
 template <typename OffT>
-static cudaError_t enqueue(ispan_ctx *c, Run<OffT> r, Ext<OffT> x, bool times) {
+static cudaError_t enqueue(ispan_ctx *c, Run<OffT> r, Ext<OffT> x, bool times, bool capturing) {
     cudaStream_t s = c->stream;
     const int G = c->g_stream;
     unsigned long long *ctl = c->ctlblk;
     cudaError_t e;
 #define EV(i) \
-    if (times) { e = cudaEventRecord(c->ev[i], s); if (e) return e; }
+    if (times) { e = cudaEventRecordWithFlags(c->ev[i], s, capturing ? cudaEventRecordExternal : 0); if (e) return e; }
 #define LK(...) \
     do { __VA_ARGS__; e = cudaGetLastError(); if (e) return e; } while (0)
     EV(0);
@@ -343,8 +346,35 @@ static int run_t(ispan_ctx *c, int64_t V, int64_t E, int32_t nseg, const OffT *f
     memset(&x, 0, sizeof(x));
     fill_run<OffT>(c, r, x, V, E, nseg, fwb, bwb, fwa, bwa, label_dev, p);
     const uint32_t flags = p ? p->flags : 0;
+#ifdef ISPAN_CHECKED
+    const bool validate = true;
+#else
+    const bool validate = (flags & ISPAN_F_VALIDATE) || c->validate_next;
+#endif
+    c->validate_next = false;
+    if (validate) {
+        CK(cudaMemsetAsync(c->err, 0, 4 * sizeof(int), c->stream));
+        k_validate<OffT><<<c->g_stream, 256, 0, c->stream>>>(fwb, bwb, fwa, bwa, V, E, c->err + 1);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(c->h_err, c->err, 4 * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        if (c->h_err[1]) return ISPAN_ERR_ARG;
+    }
+#ifdef ISPAN_CHECKED
+    {
+        long long caps[3] = {(long long)V, (long long)E, (long long)(c->maxE / kChunk + 4)};
+        long long zero[2] = {0, 0};
+        CK(cudaMemcpyToSymbolAsync(g_vcap, &caps[0], 8, 0, cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyToSymbolAsync(g_ecap, &caps[1], 8, 0, cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyToSymbolAsync(g_qcap, &caps[2], 8, 0, cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyToSymbolAsync(g_chk, zero, 16, 0, cudaMemcpyHostToDevice, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+    }
+#endif
+    // stage events are always recorded (they are nodes of the captured graph);
+    // they are read back only when the caller asks for stage times
     const bool times = (flags & ISPAN_F_STAGE_TIMES) && st;
-    bool use_graph = !(flags & ISPAN_F_NO_GRAPH) && !c->graph_broken && !times;
+    bool use_graph = !(flags & ISPAN_F_NO_GRAPH) && !c->graph_broken;
     if (use_graph) {
         char key[256];
         snprintf(key, sizeof key, "%d|%lld|%lld|%d|%p|%p|%p|%p|%p|%d|%d|%d|%d", (int)sizeof(OffT), (long long)V,
@@ -358,7 +388,7 @@ static int run_t(ispan_ctx *c, int64_t V, int64_t E, int32_t nseg, const OffT *f
             cudaGraph_t g = nullptr;
             cudaError_t e = cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal);
             if (e == cudaSuccess) {
-                cudaError_t e2 = enqueue<OffT>(c, r, x, false);
+                cudaError_t e2 = enqueue<OffT>(c, r, x, c->have_ev, true);
                 e = cudaStreamEndCapture(c->stream, &g);
                 if (e2 != cudaSuccess) e = e2;
             }
@@ -377,12 +407,23 @@ static int run_t(ispan_ctx *c, int64_t V, int64_t E, int32_t nseg, const OffT *f
     if (use_graph) {
         CK(cudaGraphLaunch(c->gexec, c->stream));
     } else {
-        CK(enqueue<OffT>(c, r, x, times));
+        CK(enqueue<OffT>(c, r, x, c->have_ev, false));
     }
     CK(cudaMemcpyAsync(c->h_counters, c->ctlblk, kNumCounters * sizeof(unsigned long long),
                        cudaMemcpyDeviceToHost, c->stream));
     CK(cudaMemcpyAsync(c->h_err, c->err, 4 * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
+#ifdef ISPAN_CHECKED
+    {
+        long long chk[2] = {0, 0};
+        CK(cudaMemcpyFromSymbol(chk, g_chk, 16));
+        if (chk[0]) {
+            fprintf(stderr, "ispan_b200 (checked build): range check failed at site %lld, index %lld\n", chk[0],
+                    chk[1]);
+            return ISPAN_ERR_INTERNAL;
+        }
+    }
+#endif
     if (c->h_err[0]) return c->h_err[0] < 0 ? c->h_err[0] : ISPAN_ERR_INTERNAL;
     if (st) {
         const unsigned long long *k = c->h_counters;
@@ -400,7 +441,9 @@ static int run_t(ispan_ctx *c, int64_t V, int64_t E, int32_t nseg, const OffT *f
         st->color_rounds = (int64_t)k[C_COLOR_ROUNDS];
         st->local_wcc = (int64_t)k[C_LOCAL_WCC];
         st->trim_rounds = (int64_t)k[C_TRIM_ROUNDS];
-        st->residual = 0;
+        st->residual = (int64_t)(k[C_ACTIVE0] - k[C_GIANT]);
+        st->fw_edges = (int64_t)k[C_FW_XDEG];
+        st->bw_edges = (int64_t)k[C_BW_XDEG];
         st->scc_count = (int64_t)(k[C_TRIM1] + k[C_TRIM2] / 2 + k[C_TRIM3] / 3 + k[C_MICE_SCC] + k[C_GIANTS]);
         if (times) {
             float ms[12];
@@ -525,13 +568,17 @@ static int run_common(ispan_ctx *c, const ispan_csr *g, int32_t nseg, const int6
     } else {
         vb = {0, g->V};
     }
-    CK(cudaMemcpyAsync(c->vbase, vb.data(), vb.size() * sizeof(int64_t), cudaMemcpyHostToDevice, c->stream));
-    CK(cudaStreamSynchronize(c->stream));  // vb is a host temporary
+    if (vb != c->vbase_host) {  // upload only when the segmentation changed
+        CK(cudaMemcpyAsync(c->vbase, vb.data(), vb.size() * sizeof(int64_t), cudaMemcpyHostToDevice, c->stream));
+        CK(cudaStreamSynchronize(c->stream));  // vb is a host temporary
+        c->vbase_host = vb;
+    }
     const void *fwb = g->fw_beg, *bwb = g->bw_beg;
     const int32_t *fwa = g->fw_adj, *bwa = g->bw_adj;
     if (!g->on_device) {
         if ((rc = check_host_offsets(g))) return rc;
         if ((rc = upload(c, g))) return rc;
+        c->validate_next = true;  // adjacency ids of host input are checked on the device
         fwb = c->up_fw_beg;
         bwb = c->up_bw_beg;
         fwa = c->up_fw_adj;

@@ -63,10 +63,35 @@ __device__ void compact_words(int64_t W, WordFn f, int32_t *out, unsigned long l
             if (i < warp) off += s_warp[i];
             all += s_warp[i];
         }
-        if ((m >> lane) & 1u) out[run + off + __popc(m & lanemask_lt())] = (int32_t)(wi * 32 + lane);
+        if ((m >> lane) & 1u) {
+            int64_t at = run + off + __popc(m & lanemask_lt());
+            if (VOK(at, 13)) out[at] = (int32_t)(wi * 32 + lane);
+        }
         run += all;
         __syncthreads();
     }
+}
+
+// ---------------------------------------------------------------------------
+// Input check on the device: offsets monotone from 0 to E, every adjacency
+// id in [0, V).  The reference's loader trusts its files (src/graph.cpp:2-92);
+// here a malformed CSR is reported as ISPAN_ERR_ARG before any stage reads it.
+template <typename OffT>
+__global__ void k_validate(const OffT *fb, const OffT *bb, const int32_t *fa, const int32_t *ba, int64_t V,
+                           int64_t E, int *bad) {
+    const int64_t gt = (int64_t)blockIdx.x * blockDim.x + threadIdx.x, nt = (int64_t)gridDim.x * blockDim.x;
+    int err = 0;
+    for (int64_t i = gt; i <= V; i += nt) {
+        int64_t a = fb[i], b = bb[i];
+        if (i == 0 && (a != 0 || b != 0)) err = 1;
+        if (i == V && (a != E || b != E)) err = 1;
+        if (i < V && (fb[i + 1] < a || bb[i + 1] < b)) err = 1;
+    }
+    for (int64_t e = gt; e < E; e += nt) {
+        int32_t x = fa[e], y = ba[e];
+        if (x < 0 || x >= V || y < 0 || y >= V) err = 1;
+    }
+    if (__syncthreads_or(err) && threadIdx.x == 0) atomicExch(bad, 1);
 }
 
 // ---------------------------------------------------------------------------
@@ -161,9 +186,11 @@ __global__ void k_seed(Run<OffT> r) {
                 other = ld_off(r.bw_beg, p + 1) - ld_off(r.bw_beg, p);
                 atomicAdd(r.counters + C_FW_SIZE, 1ull);
                 atomicAdd(r.counters + C_FW_MU, (unsigned long long)other);
+                atomicAdd(r.counters + C_FW_XDEG, (unsigned long long)dg);
             } else {
                 set_bit(r.B, p);
                 dg = ld_off(r.bw_beg, p + 1) - ld_off(r.bw_beg, p);
+                atomicAdd(r.counters + C_BW_XDEG, (unsigned long long)dg);
             }
         }
         q_append(ok, (int32_t)p, dg, r.qv[0], r.qe[0], r.qchunk[0], r.qpk, r.V);
@@ -234,7 +261,7 @@ __device__ __forceinline__ void count_active(const OffT *beg, const int32_t *adj
     int64_t e0 = ld_off(beg, v), e1 = ld_off(beg, v + 1);
     int c = 0;
     for (int64_t e = e0; e < e1; ++e) {
-        int32_t w = __ldg(adj + e);
+        int32_t w = ld_adj(adj, e);
         c += (w != v) && bitc(A, w);
     }
     n = c;
@@ -295,7 +322,7 @@ __global__ void __launch_bounds__(kBlock) k_trim1(Run<OffT> r, Ext<OffT> x, int 
                     bool nd = false;
                     int32_t w = 0;
                     if (k < len) {
-                        w = __ldg(adj + e0 + k);
+                        w = ld_adj(adj, e0 + k);
                         if (w != t && bitc(r.A, w) && !bitv(r.D, w)) {
                             if (atomicSub(cnt + w, 1) == 1) nd = set_bit(r.D, w);
                         }
@@ -343,7 +370,7 @@ __device__ __forceinline__ int distinct_active(const OffT *beg, const int32_t *a
     int64_t e0 = ld_off(beg, v), e1 = ld_off(beg, v + 1);
     int d = 0;
     for (int64_t e = e0; e < e1; ++e) {
-        int32_t w = __ldg(adj + e);
+        int32_t w = ld_adj(adj, e);
         if (w == x1 || w == x2 || !bitv(A, w)) continue;
         if (d == 0) { n1 = w; d = 1; }
         else if (d == 1 && w != n1) { n2 = w; d = 2; }
@@ -448,6 +475,18 @@ __device__ __forceinline__ int32_t uf_find(int32_t *parent, int32_t x) {
     return x;
 }
 
+// Read-only root walk for the flatten pass: once hooking is over, path
+// halving must not run concurrently with the final `parent[v] = root` writes,
+// or a halving store could replace a final root with an intermediate ancestor.
+__device__ __forceinline__ int32_t uf_root(const int32_t *parent, int32_t x) {
+    int32_t p = __ldcg(parent + x);
+    while (p != x) {
+        x = p;
+        p = __ldcg(parent + x);
+    }
+    return x;
+}
+
 template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_wcc_init(Run<OffT> r, Ext<OffT> x, int in) {
     const int64_t n = (int64_t)__ldcg(x.ctl + K_WL0 + in);
@@ -467,7 +506,7 @@ __global__ void __launch_bounds__(kBlock) k_wcc_hook(Run<OffT> r, Ext<OffT> x, i
         int32_t v = r.wl[in][i];
         int64_t e0 = ld_off(r.fw_beg, v), e1 = ld_off(r.fw_beg, v + 1);
         for (int64_t e = e0; e < e1; ++e) {
-            int32_t w = __ldg(r.fw_adj + e);
+            int32_t w = ld_adj(r.fw_adj, e);
             if (w == v || !bitc(r.A, w)) continue;
             int32_t a = v, b = w;
             for (int guard = 0; guard < (1 << 20); ++guard) {
@@ -493,7 +532,7 @@ __global__ void __launch_bounds__(kBlock) k_wcc_flatten(Run<OffT> r, Ext<OffT> x
         int32_t v = 0;
         if (i < n) {
             v = r.wl[in][i];
-            int32_t root = uf_find(r.parent, v);
+            int32_t root = uf_root(r.parent, v);
             r.parent[v] = root;
             isroot = root == v;
             // warp-aggregate the member count per distinct root
@@ -538,7 +577,7 @@ __global__ void __launch_bounds__(kBlock) k_wcc_scatter(Run<OffT> r, Ext<OffT> x
             int32_t b = r.aux2[root];
             if (b >= 0) {
                 int32_t k = atomicAdd(r.cnt_out + root, 1);
-                r.members[b + k] = v;
+                if (VOK((long long)b + k, 15)) r.members[b + k] = v;
                 r.cnt_in[v] = k;  // local index inside the WCC
             } else {
                 big = true;
@@ -568,6 +607,7 @@ __global__ void __launch_bounds__(kLocalThreads) k_local_scc(Run<OffT> r, Ext<Of
     for (int64_t wq = blockIdx.x; wq < nsmall; wq += gridDim.x) {
         const int32_t root = x.small[wq];
         const int32_t nv = r.aux[root];
+        if (!ICHK(nv >= 1 && nv <= kLocalV, 17, nv)) continue;
         const int32_t base = r.aux2[root];
         // per-vertex internal out-degree, then a vertex-order scan by warp 0
         for (int i = threadIdx.x; i < nv; i += kLocalThreads) {
@@ -576,7 +616,7 @@ __global__ void __launch_bounds__(kLocalThreads) k_local_scc(Run<OffT> r, Ext<Of
             int32_t dcount = 0;
             int64_t e0 = ld_off(r.fw_beg, u), e1 = ld_off(r.fw_beg, u + 1);
             for (int64_t e = e0; e < e1; ++e) {
-                int32_t w = __ldg(r.fw_adj + e);
+                int32_t w = ld_adj(r.fw_adj, e);
                 dcount += (w != u) && bitc(r.A, w);
             }
             loff[i + 1] = dcount;
@@ -602,7 +642,7 @@ __global__ void __launch_bounds__(kLocalThreads) k_local_scc(Run<OffT> r, Ext<Of
             // spill: hand the whole WCC to the colouring path
             for (int i = threadIdx.x; i < nv; i += kLocalThreads) {
                 unsigned long long p = atomicAdd(x.ctl + K_LARGE, 1ull);
-                x.large[0][p] = gid[i];
+                if (VOK((long long)p, 16)) x.large[0][p] = gid[i];
             }
             if (threadIdx.x == 0) atomicAdd(r.counters + C_SPILL, 1ull);
             __syncthreads();
@@ -615,8 +655,12 @@ __global__ void __launch_bounds__(kLocalThreads) k_local_scc(Run<OffT> r, Ext<Of
                 int32_t p = loff[i];
                 int64_t e0 = ld_off(r.fw_beg, u), e1 = ld_off(r.fw_beg, u + 1);
                 for (int64_t e = e0; e < e1; ++e) {
-                    int32_t w = __ldg(r.fw_adj + e);
-                    if (w != u && bitc(r.A, w)) ladj[p++] = (uint16_t)r.cnt_in[w];
+                    int32_t w = ld_adj(r.fw_adj, e);
+                    if (w != u && bitc(r.A, w)) {
+                        int32_t li = r.cnt_in[w];
+                        if (ICHK(p < kLocalE && li >= 0 && li < nv, 14, ((long long)p << 32) | (li & 0xffffffff)))
+                            ladj[p++] = (uint16_t)li;
+                    }
                 }
             }
         }
@@ -738,7 +782,7 @@ __global__ void __launch_bounds__(kBlock) k_color(Run<OffT> r, Ext<OffT> x) {
                     bool push = false;
                     int32_t w = 0;
                     if (k < len) {
-                        w = __ldg(r.fw_adj + e0 + k);
+                        w = ld_adj(r.fw_adj, e0 + k);
                         if (w != v && bitv(r.A, w) && c < __ldcg(col + w)) {
                             int32_t old = atomicMin(col + w, c);
                             if (c < old) {
@@ -785,7 +829,7 @@ __global__ void __launch_bounds__(kBlock) k_color(Run<OffT> r, Ext<OffT> x) {
                     bool push = false;
                     int32_t u = 0;
                     if (k < len) {
-                        u = __ldg(r.bw_adj + e0 + k);
+                        u = ld_adj(r.bw_adj, e0 + k);
                         if (u != v && bitv(r.A, u) && __ldcg(col + u) == c && !bitv(r.F, u)) push = set_bit(r.F, u);
                     }
                     wl_append(push, u, qn, cqc + (lv + 1) % 3);

@@ -1,0 +1,74 @@
+"""GPU generators: well-formed CSR, the intended SCC structure, and GPU
+pipeline labels equal to the oracle on scaled-down versions of the benchmark
+graphs."""
+import numpy as np
+import pytest
+
+import oracle
+from ispan_b200 import Context, gen, graphs as G
+
+pytestmark = pytest.mark.gpu
+
+
+def exact_check(csr, **kw):
+    with Context(csr.V, csr.E) as ctx:
+        labels, st = ctx.run_csr(csr, histogram=True, **kw)
+    exact = oracle.tarjan(csr)
+    assert np.array_equal(labels, exact)
+    assert st["histogram"] == oracle.histogram(exact)
+    return exact, st
+
+
+def test_rmat_matches_numpy_shape():
+    g = gen.rmat(12, 16, 3)
+    csr = g.to_host(np.int32)
+    G.validate(csr)
+    assert csr.V == 4096 and 0.8 * 16 * 4096 < csr.E <= 16 * 4096
+    exact_check(csr)
+
+
+def test_social_small_structure_and_parity():
+    g = gen.social(seed=2, scale=0.005)
+    csr = g.to_host(np.int64)
+    G.validate(csr)
+    exact, st = exact_check(csr)
+    hist = oracle.histogram(exact)
+    big = max(hist)
+    assert abs(big / csr.V - 0.80) < 0.02          # giant SCC ~80 % of vertices
+    assert hist.get(2, 0) >= 0.9 * int(80112 * 0.005)  # planted 2-cycles survive as SCCs
+    lab0 = exact[0]
+    assert (exact == lab0).sum() == big             # vertex 0 is in the giant SCC
+
+
+def test_web_small_parity():
+    g = gen.web(seed=3, scale=0.0005)
+    csr = g.to_host(np.int64)
+    G.validate(csr)
+    exact, st = exact_check(csr)
+    hist = oracle.histogram(exact)
+    assert max(hist) > 0.3 * csr.V
+
+
+def test_batch_small_parity():
+    g = gen.batch(nseg=24, vmin=100, vmax=5000, ef_min=4, ef_max=12, max_cycle=40, seed=5)
+    csr = g.to_host(np.int32)
+    G.validate(csr)
+    with Context(csr.V, csr.E) as ctx:
+        labels, st = ctx.run_csr(csr, vbase=g.vbase, histogram=True)
+    exact = oracle.tarjan(csr)
+    assert np.array_equal(labels, exact)
+    # labels never cross graph boundaries
+    seg = np.searchsorted(g.vbase, np.arange(csr.V), side="right") - 1
+    assert np.array_equal(seg, np.searchsorted(g.vbase, labels, side="right") - 1)
+
+
+def test_social_medium_repeated_runs_exact():
+    """Repeated runs on one context (graph replay, state left by the previous
+    run) stay exact on a 2 %-scale social graph."""
+    g = gen.social(seed=4, scale=0.02)
+    csr = g.to_host(np.int64)
+    exact = oracle.tarjan(csr)
+    with Context(csr.V, csr.E) as ctx:
+        for use_graph in (False, True, True, True):
+            labels, st = ctx.run_csr(csr, use_graph=use_graph)
+            assert np.array_equal(labels, exact)
