@@ -65,6 +65,7 @@ typedef struct {
 #define ISPAN_F_NO_L2_WINDOW 8u     /* do not pin the status maps in L2 */
 #define ISPAN_F_VALIDATE 16u        /* check a device-resident CSR before the run
                                        (host CSRs are always checked) */
+#define ISPAN_F_EXACT_STATS 32u     /* also fill fw_edges / bw_edges (one extra pass) */
 
 /* Stage-time slots follow the reference's avg_time[15] meanings
  * (src/scc_core.cpp:24-25, :1037-1053): 0 trim, 1 elephant SCC, 2 mice SCC,
@@ -77,8 +78,8 @@ typedef struct {
     int64_t n_trim1, n_trim2, n_trim3; /* vertices labelled by each trim */
     int64_t n_mice_vertices, n_mice_scc, n_wcc;
     int64_t fw_size, fw_levels, bw_levels, residual, color_rounds, local_wcc, trim_rounds;
-    int64_t fw_edges;         /* sum of out-degrees over the forward set F */
-    int64_t bw_edges;         /* sum of in-degrees over the pivot SCC(s) S */
+    int64_t fw_edges;         /* sum of out-degrees over the forward set F (ISPAN_F_EXACT_STATS) */
+    int64_t bw_edges;         /* sum of in-degrees over the pivot SCC(s) S (ISPAN_F_EXACT_STATS) */
     /* sparse size histogram: pairs (hist_size[i], hist_count[i]) sorted by
      * size; the caller supplies the arrays (hist_cap entries) or NULLs */
     int64_t *hist_size, *hist_count;
@@ -117,6 +118,13 @@ int ispan_scc_run_batch(ispan_ctx *ctx, const ispan_csr *g, int32_t nseg, const 
  * codes_out has V+1 entries, the last (the reference's phantom slot) 0.
  * Valid after the most recent run on ctx; host memory. */
 int ispan_ref_codes(ispan_ctx *ctx, int32_t *codes_out);
+
+/* Diagnostics: per-level trace of the two reachability searches of the last
+ * run, [2][256][4] int64 (direction, level): mode (0 top-down, 1 bottom-up,
+ * 2 small-frontier tail), vertices reached, frontier edges, %globaltimer ns.
+ * No counterpart in the reference (its VERBOSE "Level-k" lines, src/fw_bw.h:557-572,
+ * print the same kind of record). */
+int ispan_debug_trace(ispan_ctx *ctx, int64_t *out, int64_t cap);
 
 const char *ispan_strerror(int code);
 /* library version string */

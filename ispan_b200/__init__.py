@@ -80,7 +80,7 @@ class Context:
 
     def run(self, fw_beg, fw_adj, bw_beg, bw_adj, V: int | None = None, labels_out=None,
             vbase=None, alpha=30, beta=200, gamma=10, theta=0.1, stage_times=False, use_graph=True,
-            histogram=False):
+            histogram=False, exact_stats=False, validate=False):
         """Detect SCCs.  Arrays are numpy (host) or torch CUDA tensors (device);
         offsets int32 or int64, ids int32.  Returns (labels, stats): labels[V]
         int32 canonical min-id labels, a numpy array for host input or the
@@ -99,6 +99,10 @@ class Context:
             flags |= _lib.F_STAGE_TIMES
         if not use_graph:
             flags |= _lib.F_NO_GRAPH
+        if exact_stats:
+            flags |= _lib.F_EXACT_STATS
+        if validate:
+            flags |= _lib.F_VALIDATE
         if on_dev:
             import torch
             if labels_out is None:
@@ -131,6 +135,18 @@ class Context:
 
     def run_csr(self, csr: CSR, **kw):
         return self.run(csr.fw_beg, csr.fw_adj, csr.bw_beg, csr.bw_adj, V=csr.V, **kw)
+
+    def trace(self):
+        """Per-level records of the last run's FW and BW searches: lists of
+        (mode, reached, frontier_edges, t_ns) for each direction."""
+        t = np.zeros(2 * 256 * 4, np.int64)
+        check(_lib.lib().ispan_debug_trace(self._h, t.ctypes.data, len(t)), "ispan_debug_trace")
+        t = t.reshape(2, 256, 4)
+        out = []
+        for d in range(2):
+            rows = [tuple(int(x) for x in r) for r in t[d] if r[3] != 0]
+            out.append(rows)
+        return out
 
     def ref_codes(self, V: int) -> np.ndarray:
         """scc_id codes of the last run in the reference's convention, [V+1]."""

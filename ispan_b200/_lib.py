@@ -22,6 +22,7 @@ F_NO_GRAPH = 2
 F_STAGE_TIMES = 4
 F_NO_L2_WINDOW = 8
 F_VALIDATE = 16
+F_EXACT_STATS = 32
 
 
 class IspanError(RuntimeError):
@@ -76,6 +77,7 @@ def lib() -> C.CDLL:
         L.ispan_scc_run_batch.argtypes = [P, C.POINTER(Csr), C.c_int32, P, C.POINTER(Params), P,
                                           C.POINTER(Stats)]
         L.ispan_ref_codes.argtypes = [P, P]
+        L.ispan_debug_trace.argtypes = [P, P, C.c_int64]
         L.ispan_strerror.argtypes = [C.c_int]
         L.ispan_strerror.restype = C.c_char_p
         L.ispan_version.restype = C.c_char_p
@@ -84,7 +86,7 @@ def lib() -> C.CDLL:
 
 
 SYMBOLS = ("ispan_ctx_create", "ispan_ctx_destroy", "ispan_ctx_set_stream", "ispan_ctx_bytes", "ispan_scc_run",
-           "ispan_scc_run_batch", "ispan_ref_codes", "ispan_strerror", "ispan_version")
+           "ispan_scc_run_batch", "ispan_ref_codes", "ispan_debug_trace", "ispan_strerror", "ispan_version")
 
 
 def check(rc: int, what: str = "") -> None:

@@ -12,7 +12,7 @@ namespace ispan {
 
 constexpr int kBlock = 512;           // threads per CTA for persistent stages
 constexpr int kWarps = kBlock / 32;
-constexpr int kChunk = 4096;          // edges per top-down work chunk (8 per thread)
+constexpr int kChunk = 2048;          // edges per top-down work chunk (4 per thread)
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kCountBits = 31;        // packed queue counter: count | edges << 31
 constexpr uint64_t kCountMask = (1ull << kCountBits) - 1;
@@ -61,6 +61,7 @@ struct Run {
     unsigned long long *counters; // [kNumCounters] statistics
     int64_t *hist;                // [kHistCap] SCC size histogram (sizes < cap)
     unsigned int *gsync;          // [2] grid barrier (count, generation)
+    long long *trace;             // [2][kTraceLevels][4] per-level BFS trace (diagnostics)
     int *err;                     // [4] error word, detail
     int32_t alpha, beta, gamma;
     uint32_t flags;
@@ -93,6 +94,7 @@ enum Counter {
     kNumCounters = 32
 };
 constexpr int kHistCap = 1 << 16;   // exact histogram for SCC sizes below this
+constexpr int kTraceLevels = 256;   // levels recorded per search in the diagnostics trace
 constexpr int kBigCap = 1 << 16;    // list of larger SCC sizes (hist[kHistCap..])
 
 // error codes mirror ispan_b200.h
@@ -245,6 +247,11 @@ __device__ __forceinline__ void st_release_u32(unsigned *p, unsigned v) {
     asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 __device__ __forceinline__ int ld_volatile_int(const int *p) { return *(volatile const int *)p; }
+__device__ __forceinline__ unsigned atom_add_acqrel_u32(unsigned *p, unsigned v) {
+    unsigned old;
+    asm volatile("atom.add.acq_rel.gpu.global.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
+}
 
 __device__ __noinline__ bool grid_sync(unsigned *gs, int *err) {
     __shared__ int s_ok;
@@ -252,25 +259,27 @@ __device__ __noinline__ bool grid_sync(unsigned *gs, int *err) {
     if (threadIdx.x == 0) {
         int ok = ld_volatile_int(err) == 0;
         unsigned gen = ld_acquire_u32(gs + 1);
-        __threadfence();
-        unsigned arrived = atomicAdd(gs, 1u);
+        // the CTA's writes (ordered before this thread by bar.sync) are made
+        // visible at gpu scope, then the arrival is an acq_rel atomic
+        asm volatile("fence.acq_rel.gpu;" ::: "memory");
+        unsigned arrived = atom_add_acqrel_u32(gs, 1u);
         if (arrived == gridDim.x - 1) {
             atomicExch(gs, 0u);
-            __threadfence();
             st_release_u32(gs + 1, gen + 1);
         } else {
             uint64_t t0 = globaltimer();
+            int spin = 0;
             while (ld_acquire_u32(gs + 1) == gen) {
-                if (ld_volatile_int(err) != 0) { ok = 0; break; }
-                __nanosleep(64);
-                if (globaltimer() - t0 > kBarrierTimeoutNs) {
-                    atomicCAS(err, 0, kErrTimeout);
-                    ok = 0;
-                    break;
+                if ((++spin & 63) == 0) {
+                    if (ld_volatile_int(err) != 0) { ok = 0; break; }
+                    if (globaltimer() - t0 > kBarrierTimeoutNs) {
+                        atomicCAS(err, 0, kErrTimeout);
+                        ok = 0;
+                        break;
+                    }
                 }
             }
         }
-        __threadfence();
         if (ld_volatile_int(err) != 0) ok = 0;
         s_ok = ok;
     }

@@ -158,6 +158,7 @@ enum SocCat : uint32_t {
 };
 struct SocProg {
     Perm perm;
+    Perm ring;  // order of the Hamiltonian cycle over the core ranks
     uint64_t seed;
     int64_t n_core, n_src, n_snk, n_up, n_dn, n_pair, n_tri, n_tail_v, n_tail;
     int64_t b_src, b_snk, b_up, b_dn, b_pair, b_tri, b_tail;  // rank bases
@@ -180,7 +181,11 @@ __global__ void k_social(SocProg P, uint64_t *keys, int64_t total) {
         const uint64_t s = P.seed;
         uint64_t key = 0;
         switch (cat) {
-            case S_RING: key = key_of(P.perm, j, (j + 1) % P.n_core); break;
+            case S_RING: {  // ring position j -> j+1 in an independent order of the core
+                int64_t a = P.ring.vertex(j), b = P.ring.vertex((j + 1) % P.n_core);
+                key = key_of(P.perm, a, b);
+                break;
+            }
             case S_CL:
                 key = key_of(P.perm, P.pl_out.sample(u01(rnd(s, cat, j, 0))), P.pl_in.sample(u01(rnd(s, cat, j, 1))));
                 break;
@@ -559,6 +564,7 @@ int ispan_gen_social(int device, int64_t n, int64_t edges, double giant_frac, do
     P.n_pair = n_pair;
     P.n_tri = n_tri;
     P.n_core = (int64_t)(giant_frac * n);
+    P.ring = Perm::make(P.n_core, seed ^ 0x21f6ull);
     int64_t n_triv = n - P.n_core - 2 * n_pair - 3 * n_tri - P.n_tail_v;
     if (P.n_core < 2 || n_triv < 16) return -1;
     P.n_src = n_triv * 45 / 100;

@@ -81,6 +81,7 @@ struct ispan_ctx {
     unsigned int *gsync = nullptr;
     int *err = nullptr;
     BfsCtl *bfsctl = nullptr;
+    long long *trace = nullptr;
     int64_t *vbase = nullptr;
     unsigned long long *pivot_key = nullptr, *gsize = nullptr;
     int32_t *gmin = nullptr;
@@ -169,6 +170,7 @@ static int ctx_alloc(ispan_ctx *c) {
     rc |= dalloc(&c->gsync, 4, o);
     rc |= dalloc(&c->err, 4, o);
     rc |= dalloc(&c->bfsctl, 1, o);
+    rc |= dalloc(&c->trace, 2 * kTraceLevels * 4, o);
     return rc ? ISPAN_ERR_NOMEM : ISPAN_OK;
 }
 
@@ -243,6 +245,7 @@ static void fill_run(ispan_ctx *c, Run<OffT> &r, Ext<OffT> &x, int64_t V, int64_
     r.hist = c->hist;
     r.gsync = c->gsync;
     r.err = c->err;
+    r.trace = c->trace;
     r.alpha = p && p->alpha > 0 ? p->alpha : 30;
     r.beta = p && p->beta > 0 ? p->beta : 200;
     r.gamma = p && p->gamma > 0 ? p->gamma : 10;
@@ -278,6 +281,7 @@ static cudaError_t enqueue(ispan_ctx *c, Run<OffT> r, Ext<OffT> x, bool times, b
     if ((e = cudaMemsetAsync(c->hist, 0, (kHistCap + kBigCap) * sizeof(int64_t), s))) return e;
     if ((e = cudaMemsetAsync(c->gsync, 0, 4 * sizeof(unsigned), s))) return e;
     if ((e = cudaMemsetAsync(c->err, 0, 4 * sizeof(int), s))) return e;
+    if ((e = cudaMemsetAsync(c->trace, 0, 2 * kTraceLevels * 4 * sizeof(long long), s))) return e;
     if ((e = cudaMemsetAsync(c->pivot_key, 0, r.nseg * sizeof(unsigned long long), s))) return e;
     if ((e = cudaMemsetAsync(c->gsize, 0, r.nseg * sizeof(unsigned long long), s))) return e;
     if ((e = cudaMemsetAsync(c->gmin, 0x7f, r.nseg * sizeof(int32_t), s))) return e;
@@ -290,6 +294,7 @@ static cudaError_t enqueue(ispan_ctx *c, Run<OffT> r, Ext<OffT> x, bool times, b
     if ((e = cudaMemsetAsync(r.lvl, 0, 16 * sizeof(unsigned long long), s))) return e;
     LK((k_seed<OffT, 1><<<std::max<int64_t>(1, (r.nseg + 1023) / 1024), 32 * 32, 0, s>>>(r)));
     if ((e = launch_coop(k_bfs<OffT, 1>, c->g_coop[1], s, r, c->bfsctl))) return e;
+    if (r.flags & ISPAN_F_EXACT_STATS) LK((k_reach_degrees<OffT><<<G, kBlock, 0, s>>>(r)));
     EV(3);
     LK((k_giant<OffT><<<G, kBlock, 0, s>>>(r, x)));
     LK((k_residual<OffT><<<G, kBlock, 0, s>>>(r, x)));
@@ -377,9 +382,9 @@ static int run_t(ispan_ctx *c, int64_t V, int64_t E, int32_t nseg, const OffT *f
     bool use_graph = !(flags & ISPAN_F_NO_GRAPH) && !c->graph_broken;
     if (use_graph) {
         char key[256];
-        snprintf(key, sizeof key, "%d|%lld|%lld|%d|%p|%p|%p|%p|%p|%d|%d|%d|%d", (int)sizeof(OffT), (long long)V,
+        snprintf(key, sizeof key, "%d|%lld|%lld|%d|%p|%p|%p|%p|%p|%d|%d|%d|%p|%u", (int)sizeof(OffT), (long long)V,
                  (long long)E, nseg, (const void *)fwb, (const void *)bwb, (const void *)fwa, (const void *)bwa,
-                 (void *)label_dev, r.alpha, r.beta, r.gamma, (int)(uintptr_t)c->stream);
+                 (void *)label_dev, r.alpha, r.beta, r.gamma, (void *)c->stream, r.flags & ISPAN_F_EXACT_STATS);
         if (!c->gexec || strcmp(key, c->gkey) != 0) {
             if (c->gexec) {
                 cudaGraphExecDestroy(c->gexec);
@@ -701,6 +706,14 @@ int ispan_ref_codes(ispan_ctx *c, int32_t *codes) {
         }
     }
     codes[V] = 0;
+    return ISPAN_OK;
+}
+
+int ispan_debug_trace(ispan_ctx *c, int64_t *out, int64_t cap) {
+    if (!c || !out) return ISPAN_ERR_ARG;
+    std::lock_guard<std::mutex> lock(c->mu);
+    int64_t n = std::min<int64_t>(cap, 2 * kTraceLevels * 4);
+    CK(cudaMemcpy(out, c->trace, n * sizeof(int64_t), cudaMemcpyDeviceToHost));
     return ISPAN_OK;
 }
 

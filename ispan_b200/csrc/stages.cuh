@@ -186,11 +186,9 @@ __global__ void k_seed(Run<OffT> r) {
                 other = ld_off(r.bw_beg, p + 1) - ld_off(r.bw_beg, p);
                 atomicAdd(r.counters + C_FW_SIZE, 1ull);
                 atomicAdd(r.counters + C_FW_MU, (unsigned long long)other);
-                atomicAdd(r.counters + C_FW_XDEG, (unsigned long long)dg);
             } else {
                 set_bit(r.B, p);
                 dg = ld_off(r.bw_beg, p + 1) - ld_off(r.bw_beg, p);
-                atomicAdd(r.counters + C_BW_XDEG, (unsigned long long)dg);
             }
         }
         q_append(ok, (int32_t)p, dg, r.qv[0], r.qe[0], r.qchunk[0], r.qpk, r.V);
@@ -742,9 +740,15 @@ __global__ void __launch_bounds__(kBlock) k_color(Run<OffT> r, Ext<OffT> x) {
     unsigned long long *cqc = x.ctl + K_CQ0;
     int cur = 0;
     int rounds = 0;
+    int64_t prev_n = INT64_MAX;
     for (int guard = 0; guard < (1 << 30); ++guard) {
         const int64_t n = (int64_t)__ldcg(x.ctl + (cur == 0 ? K_LARGE : K_LARGE2));
         if (n == 0) break;
+        if (n >= prev_n) {  // every round labels at least the minimum vertex's SCC
+            if (threadIdx.x == 0) atomicCAS(r.err, 0, kErrOverflow);
+            return;
+        }
+        prev_n = n;
         ++rounds;
         const int32_t *L = x.large[cur];
         if (blockIdx.x == 0 && threadIdx.x == 0) {

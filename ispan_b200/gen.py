@@ -101,8 +101,10 @@ def rmat(scale=16, edge_factor=16, seed=1, a=0.57, b=0.19, c=0.19, permute=False
                "ispan_gen_rmat")
 
 
-# Twitter-shaped stand-in: sizes of paper Table II (TW), synthetic content
-SOCIAL_TW = dict(n=41_652_231, edges=1_490_000_000, giant_frac=0.8038, gamma_out=2.1, gamma_in=1.9,
+# Twitter-shaped stand-in: sizes of paper Table II (TW), synthetic content.
+# `edges` counts sampled edges; duplicates among hub pairs are dropped, which
+# leaves ~1.47 B distinct edges at full size.
+SOCIAL_TW = dict(n=41_652_231, edges=1_735_000_000, giant_frac=0.8038, gamma_out=2.1, gamma_in=1.9,
                  n_pair=80_112, n_tri=12_198, n_tail=5_320, max_tail=1000)
 
 
