@@ -68,31 +68,6 @@ struct BfsDir {
     __device__ __forceinline__ int64_t odeg(int64_t v) const { return ld_off(obeg, v + 1) - ld_off(obeg, v); }
 };
 
-// Warp-aggregated append of up to kPer (vertex, degree) items per lane, one
-// 64-bit atomic per warp; returns each lane's first slot and edge base.
-__device__ __forceinline__ void q_reserve(int n, int64_t dsum, unsigned long long *pk, int64_t &slot0,
-                                          int64_t &eb0) {
-    const int lane = lane_id();
-    int64_t packed = ((int64_t)n) | (dsum << 20);  // n <= 8, dsum < 2^43 per lane
-    int ni = n;
-    int64_t di = dsum;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        int yn = __shfl_up_sync(kFull, ni, o);
-        int64_t yd = __shfl_up_sync(kFull, di, o);
-        if (lane >= o) { ni += yn; di += yd; }
-    }
-    (void)packed;
-    int tn = __shfl_sync(kFull, ni, 31);
-    int64_t td = __shfl_sync(kFull, di, 31);
-    unsigned long long base = 0;
-    if (tn && lane == 31)
-        base = atomicAdd(pk, ((unsigned long long)td << kCountBits) | (unsigned long long)tn);
-    base = __shfl_sync(kFull, base, 31);
-    slot0 = (int64_t)(base & kCountMask) + (ni - n);
-    eb0 = (int64_t)(base >> kCountBits) + (di - dsum);
-}
-
 // Shared staging of one chunk's queue slots (at most kChunk + 1 of them, as
 // every queued vertex has at least one edge).
 struct TdSmem {

@@ -36,6 +36,7 @@ struct Run {
     uint32_t *B;      // backward-reached (giant) / second mark map
     uint32_t *D;      // dead: claimed by a trim in the current stage
     uint32_t *P;      // snapshot of the visit map at the start of a bottom-up level
+    uint32_t *T;      // trimmed by the first pass (zero full in- or out-degree)
 
     // frontier queues (double buffered): vertex, edge prefix, chunk -> slot
     int32_t *qv[2];

@@ -5,7 +5,7 @@
 // Stage sequence (reference src/scc_core.cpp:144-1070, same order):
 //   trim-1-first + pivot      k_trim1_first, k_seed
 //   elephant FW / BW          k_bfs<.,0>, k_bfs<.,1>   (persistent, cooperative)
-//   giant, residual           k_giant, k_residual
+//   giant, residual           k_giant_residual
 //   trim-1 peel (fixpoint)    k_trim1                  (persistent, cooperative)
 //   trim-2, trim-3            k_trim2, k_trim3
 //   trim-1 peel again         k_trim1
@@ -69,7 +69,7 @@ struct ispan_ctx {
     // device scratch
     int32_t *label = nullptr;
     uint8_t *cls = nullptr;
-    uint32_t *A = nullptr, *F = nullptr, *B = nullptr, *D = nullptr, *P = nullptr;
+    uint32_t *A = nullptr, *F = nullptr, *B = nullptr, *D = nullptr, *P = nullptr, *T = nullptr;
     int32_t *qv[2] = {nullptr, nullptr};
     int64_t *qe[2] = {nullptr, nullptr};
     int32_t *qchunk[2] = {nullptr, nullptr};
@@ -128,7 +128,7 @@ extern "C" int64_t ispan_ctx_bytes(int64_t V, int64_t E) {
     int64_t W = words_of(V);
     int64_t b = 0;
     b += V * 4 + V;                 // label, cls
-    b += 5 * W * 4;                 // bitmaps
+    b += 6 * W * 4;                 // bitmaps
     b += 2 * (V * 4 + (V + 1) * 8); // queues
     b += 2 * ((E / kChunk + 4) * 4);
     b += 2 * V * 4;                 // worklists
@@ -150,6 +150,7 @@ static int ctx_alloc(ispan_ctx *c) {
     rc |= dalloc(&c->B, W, o);
     rc |= dalloc(&c->D, W, o);
     rc |= dalloc(&c->P, W, o);
+    rc |= dalloc(&c->T, W, o);
     for (int i = 0; i < 2; ++i) {
         rc |= dalloc(&c->qv[i], V, o);
         rc |= dalloc(&c->qe[i], V + 1, o);
@@ -221,7 +222,7 @@ static void fill_run(ispan_ctx *c, Run<OffT> &r, Ext<OffT> &x, int64_t V, int64_
     r.fw_adj = fwa;
     r.bw_adj = bwa;
     r.label = label;
-    r.A = c->A; r.F = c->F; r.B = c->B; r.D = c->D; r.P = c->P;
+    r.A = c->A; r.F = c->F; r.B = c->B; r.D = c->D; r.P = c->P; r.T = c->T;
     for (int i = 0; i < 2; ++i) {
         r.qv[i] = c->qv[i];
         r.qe[i] = c->qe[i];
@@ -296,8 +297,7 @@ static cudaError_t enqueue(ispan_ctx *c, Run<OffT> r, Ext<OffT> x, bool times, b
     if ((e = launch_coop(k_bfs<OffT, 1>, c->g_coop[1], s, r, c->bfsctl))) return e;
     if (r.flags & ISPAN_F_EXACT_STATS) LK((k_reach_degrees<OffT><<<G, kBlock, 0, s>>>(r)));
     EV(3);
-    LK((k_giant<OffT><<<G, kBlock, 0, s>>>(r, x)));
-    LK((k_residual<OffT><<<G, kBlock, 0, s>>>(r, x)));
+    LK((k_giant_residual<OffT><<<G, kBlock, 0, s>>>(r, x)));
     EV(4);
     if ((e = launch_coop(k_trim1<OffT>, c->g_coop[2], s, r, x, 0, 1))) return e;
     EV(5);
@@ -692,12 +692,18 @@ int ispan_ref_codes(ispan_ctx *c, int32_t *codes) {
     int64_t V = c->last_V;
     std::vector<int32_t> lab(V);
     std::vector<uint8_t> cls(V);
+    std::vector<uint32_t> tm((V + 31) / 32 + 1), bm((V + 31) / 32 + 1);
     if (V) {
         CK(cudaMemcpy(lab.data(), c->last_label, V * 4, cudaMemcpyDeviceToHost));
         CK(cudaMemcpy(cls.data(), c->cls, V, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(tm.data(), c->T, ((V + 31) / 32) * 4, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(bm.data(), c->B, ((V + 31) / 32) * 4, cudaMemcpyDeviceToHost));
     }
     for (int64_t v = 0; v < V; ++v) {
-        switch (cls[v]) {
+        // the giant and the first trim are recorded as bitmaps, later classes per vertex
+        uint8_t k = ((bm[v >> 5] >> (v & 31)) & 1u) ? (uint8_t)CLS_GIANT
+                    : ((tm[v >> 5] >> (v & 31)) & 1u) ? (uint8_t)CLS_TRIM1 : cls[v];
+        switch (k) {
             case CLS_GIANT: codes[v] = 1; break;
             case CLS_TRIM1: codes[v] = -1; break;
             case CLS_TRIM2: codes[v] = -2; break;

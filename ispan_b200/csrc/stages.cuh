@@ -20,7 +20,7 @@ enum Cls : uint8_t { CLS_NONE = 0, CLS_GIANT = 1, CLS_TRIM1 = 2, CLS_TRIM2 = 3, 
 // control-block slots (Run::ctl64): worklist and queue counters
 enum Ctl64 {
     K_WL0 = 0, K_WL1, K_CQ0, K_CQ1, K_CQ2, K_ROOTS, K_SMALL, K_LARGE, K_ALLOC, K_LARGE2,
-    K_SPILL, K_MICE_SCC, kNumCtl = 32
+    K_SPILL, K_MICE_SCC, K_LOCAL_NEXT, kNumCtl = 32
 };
 
 constexpr int kLocalV = 1024;   // a WCC up to this many vertices ...
@@ -105,52 +105,58 @@ __global__ void k_validate(const OffT *fb, const OffT *bb, const int32_t *fa, co
 template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_trim1_first(Run<OffT> r, Ext<OffT> x) {
     __shared__ int64_t sh[kWarps];
+    constexpr int U = 4;  // words per warp step: four independent offset loads in flight
     const int lane = lane_id();
     const int64_t gw = ((int64_t)blockIdx.x * kBlock + threadIdx.x) >> 5;
     const int64_t nw = (int64_t)gridDim.x * kWarps;
     int64_t n_act = 0, mu = 0, n_tr = 0;
     unsigned long long best = 0;
-    for (int64_t wi = gw; wi < r.W; wi += nw) {
-        int64_t v = wi * 32 + lane;
-        bool valid = v < r.V;
-        int64_t od = 0, id = 0;
-        if (valid) {
-            od = ld_off(r.fw_beg, v + 1) - ld_off(r.fw_beg, v);
-            id = ld_off(r.bw_beg, v + 1) - ld_off(r.bw_beg, v);
+    for (int64_t wb = gw * U; wb < r.W; wb += nw * U) {
+        int64_t od[U], id[U];
+        bool valid[U];
+#pragma unroll
+        for (int j = 0; j < U; ++j) {
+            const int64_t v = (wb + j) * 32 + lane;
+            valid[j] = (wb + j) < r.W && v < r.V;
+            od[j] = valid[j] ? ld_off(r.fw_beg, v + 1) - ld_off(r.fw_beg, v) : 0;
+            id[j] = valid[j] ? ld_off(r.bw_beg, v + 1) - ld_off(r.bw_beg, v) : 0;
         }
-        bool act = valid && od > 0 && id > 0;
-        unsigned am = __ballot_sync(kFull, act);
-        if (lane == 0) {
-            r.A[wi] = am;
-            r.F[wi] = 0;
-            r.B[wi] = 0;
-            r.D[wi] = 0;
-        }
-        if (valid && !act) {
-            r.label[v] = (int32_t)v;
-            r.cls[v] = CLS_TRIM1;
-            ++n_tr;
-        }
-        unsigned long long key = 0;
-        if (act) {
-            ++n_act;
-            mu += od;
-            unsigned long long prod = (unsigned long long)od * (unsigned long long)id;
-            if (prod > 0xffffffffull) prod = 0xffffffffull;
-            key = (prod << 32) | (0xffffffffull - (unsigned long long)v);
-        }
-        if (r.nseg == 1) {
-            best = key > best ? key : best;
-        } else {
-            // segmented: lanes of one word nearly always share a graph
-            int s = valid ? seg_of(r.vbase, r.nseg, v) : -1;
-            int s0 = __shfl_sync(kFull, s, 0);
-            bool uni = __all_sync(kFull, s == s0 || s < 0);
-            if (uni) {
-                unsigned long long m = warp_max_u64(key);
-                if (lane == 0 && m) atomicMax(r.pivot_key + s0, m);
-            } else if (key) {
-                atomicMax(r.pivot_key + s, key);
+#pragma unroll
+        for (int j = 0; j < U; ++j) {
+            const int64_t wi = wb + j;
+            const int64_t v = wi * 32 + lane;
+            const bool act = valid[j] && od[j] > 0 && id[j] > 0;
+            const unsigned am = __ballot_sync(kFull, act);
+            const unsigned tm = __ballot_sync(kFull, valid[j] && !act);
+            if (lane == 0 && wi < r.W) {
+                r.A[wi] = am;
+                r.T[wi] = tm;  // size-1 SCCs of the first trim; labelled by k_finalize
+                r.F[wi] = 0;
+                r.B[wi] = 0;
+                r.D[wi] = 0;
+            }
+            n_tr += valid[j] && !act;
+            unsigned long long key = 0;
+            if (act) {
+                ++n_act;
+                mu += od[j];
+                unsigned long long prod = (unsigned long long)od[j] * (unsigned long long)id[j];
+                if (prod > 0xffffffffull) prod = 0xffffffffull;
+                key = (prod << 32) | (0xffffffffull - (unsigned long long)v);
+            }
+            if (r.nseg == 1) {
+                best = key > best ? key : best;
+            } else {
+                // segmented: lanes of one word nearly always share a graph
+                int sg = valid[j] ? seg_of(r.vbase, r.nseg, v) : -1;
+                int s0 = __shfl_sync(kFull, sg, 0);
+                bool uni = __all_sync(kFull, sg == s0 || sg < 0);
+                if (uni) {
+                    unsigned long long m = warp_max_u64(key);
+                    if (lane == 0 && m) atomicMax(r.pivot_key + s0, m);
+                } else if (key) {
+                    atomicMax(r.pivot_key + sg, key);
+                }
             }
         }
     }
@@ -195,35 +201,42 @@ __global__ void k_seed(Run<OffT> r) {
     }
 }
 
-// The pivot SCC of each graph is B (reached backward inside F).  Leave the
-// active map, record the class, and find each graph's minimum member id (its
-// canonical label, written by k_finalize).  Warp per word.
+// The pivot SCC of each graph is B (reached backward inside F).  One pass
+// over the maps: B leaves the active map, each graph's minimum member id (its
+// canonical label, written by k_finalize) and size are taken, and the
+// remaining active vertices are compacted into the residual worklist.  Each
+// CTA owns a contiguous range of words, one word per thread per step; one
+// atomic per CTA reserves its share of the worklist.
 template <typename OffT>
-__global__ void __launch_bounds__(kBlock) k_giant(Run<OffT> r, Ext<OffT> x) {
+__global__ void __launch_bounds__(kBlock) k_giant_residual(Run<OffT> r, Ext<OffT> x) {
     __shared__ int64_t sh[kWarps];
-    const int lane = lane_id();
-    const int64_t gw = ((int64_t)blockIdx.x * kBlock + threadIdx.x) >> 5;
-    const int64_t nw = (int64_t)gridDim.x * kWarps;
-    int64_t n = 0;
+    __shared__ int s_scan[kWarps];
+    __shared__ unsigned long long s_base;
+    const int tid = threadIdx.x, lane = lane_id(), warp = tid >> 5;
+    const int64_t per = (r.W + gridDim.x - 1) / gridDim.x;
+    const int64_t w0 = min(r.W, (int64_t)blockIdx.x * per), w1 = min(r.W, w0 + per);
+    int64_t n_giant = 0, n_res = 0;
     int gm = 0x7fffffff;
-    for (int64_t wi = gw; wi < r.W; wi += nw) {
-        uint32_t s = r.B[wi];
-        if (!s) continue;
-        if (lane == 0) r.A[wi] &= ~s;
-        int64_t v = wi * 32 + lane;
-        bool me = (s >> lane) & 1u;
-        if (me) {
-            r.cls[v] = CLS_GIANT;
-            ++n;
-        }
-        if (r.nseg == 1) {
-            gm = min(gm, me ? (int)v : 0x7fffffff);
-        } else {
-            int sg = me ? seg_of(r.vbase, r.nseg, v) : -1;
-            unsigned grp = __match_any_sync(kFull, sg);
-            if (me) {
-                atomicMin(r.gmin + sg, (int)v);
-                if (lane == __ffs(grp) - 1) atomicAdd(r.gsize + sg, (unsigned long long)__popc(grp));
+    // pass 1: update A, giant stats, count the residual
+    for (int64_t wi = w0 + tid; wi < w1; wi += kBlock) {
+        uint32_t a = r.A[wi], b = r.B[wi];
+        uint32_t res = a & ~b;
+        if (b) r.A[wi] = res;
+        n_res += __popc(res);
+        if (b) {
+            n_giant += __popc(b);
+            int v0 = (int)(wi * 32 + __ffs(b) - 1);  // the word's smallest member
+            if (r.nseg == 1) {
+                gm = min(gm, v0);
+            } else {
+                for (uint32_t m = b; m;) {  // members may span graphs
+                    int bit = __ffs(m) - 1;
+                    int64_t v = wi * 32 + bit;
+                    int sg = seg_of(r.vbase, r.nseg, v);
+                    atomicMin(r.gmin + sg, (int)v);
+                    atomicAdd(r.gsize + sg, 1ull);
+                    m &= m - 1;
+                }
             }
         }
     }
@@ -231,18 +244,43 @@ __global__ void __launch_bounds__(kBlock) k_giant(Run<OffT> r, Ext<OffT> x) {
         gm = warp_min(gm);
         if (lane == 0 && gm != 0x7fffffff) atomicMin(r.gmin, gm);
     }
-    int64_t t = block_sum64(n, sh);
-    if (threadIdx.x == 0 && t) {
-        atomicAdd(r.counters + C_GIANT, (unsigned long long)t);
-        if (r.nseg == 1) atomicAdd(r.gsize, (unsigned long long)t);
+    int64_t tg = block_sum64(n_giant, sh), tr = block_sum64(n_res, sh);
+    if (tid == 0) {
+        if (tg) {
+            atomicAdd(r.counters + C_GIANT, (unsigned long long)tg);
+            if (r.nseg == 1) atomicAdd(r.gsize, (unsigned long long)tg);
+        }
+        s_base = tr ? atomicAdd(x.ctl + K_WL0, (unsigned long long)tr) : 0ull;
     }
-}
-
-// Residual worklist: every still-active vertex, in id order per CTA.
-template <typename OffT>
-__global__ void __launch_bounds__(kBlock) k_residual(Run<OffT> r, Ext<OffT> x) {
-    const uint32_t *A = r.A;
-    compact_words(r.W, [A] __device__(int64_t wi) { return A[wi]; }, r.wl[0], x.ctl + K_WL0);
+    __syncthreads();
+    // pass 2: write the residual vertices in word order
+    int64_t run = (int64_t)s_base;
+    for (int64_t wb = w0; wb < w1; wb += kBlock) {
+        int64_t wi = wb + tid;
+        uint32_t m = wi < w1 ? __ldcg(r.A + wi) : 0u;
+        int c = __popc(m), incl = c;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int y = __shfl_up_sync(kFull, incl, o);
+            if (lane >= o) incl += y;
+        }
+        if (lane == 31) s_scan[warp] = incl;
+        __syncthreads();
+        int off = 0, all = 0;
+#pragma unroll
+        for (int i = 0; i < kWarps; ++i) {
+            int t = s_scan[i];
+            off += i < warp ? t : 0;
+            all += t;
+        }
+        int64_t at = run + off + incl - c;
+        for (; m; m &= m - 1) {
+            if (VOK(at, 13)) r.wl[0][at] = (int32_t)(wi * 32 + __ffs(m) - 1);
+            ++at;
+        }
+        run += all;
+        __syncthreads();
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -601,8 +639,17 @@ __global__ void __launch_bounds__(kLocalThreads) k_local_scc(Run<OffT> r, Ext<Of
     __shared__ int16_t idx[kLocalV], low[kLocalV], stk[kLocalV], csv[kLocalV];
     __shared__ int32_t cse[kLocalV];
     __shared__ uint8_t onst[kLocalV];
+    __shared__ uint32_t fwm[kLocalV / 32], bwm[kLocalV / 32], frm[2][kLocalV / 32];
+    __shared__ int s_flag, s_min, s_both;
+    __shared__ long long s_wq;
     const int64_t nsmall = (int64_t)__ldcg(x.ctl + K_SMALL);
-    for (int64_t wq = blockIdx.x; wq < nsmall; wq += gridDim.x) {
+    for (int guard = 0; guard < (1 << 30); ++guard) {
+        // dynamic assignment: large and small WCCs interleave across CTAs
+        __syncthreads();  // everyone is done with the previous WCC (and s_wq)
+        if (threadIdx.x == 0) s_wq = (long long)atomicAdd(x.ctl + K_LOCAL_NEXT, 1ull);
+        __syncthreads();
+        const int64_t wq = s_wq;
+        if (wq >= nsmall) break;
         const int32_t root = x.small[wq];
         const int32_t nv = r.aux[root];
         if (!ICHK(nv >= 1 && nv <= kLocalV, 17, nv)) continue;
@@ -663,7 +710,78 @@ __global__ void __launch_bounds__(kLocalThreads) k_local_scc(Run<OffT> r, Ext<Of
             }
         }
         __syncthreads();
-        if (threadIdx.x == 0) {
+        // One forward and one backward search from local vertex 0, all threads
+        // on bitmaps in shared memory.  If both reach every vertex, the WCC is
+        // a single SCC (the common case for planted cycles with chords) and
+        // no serial work is needed.
+        const int nw = (nv + 31) >> 5;
+        for (int i = threadIdx.x; i < kLocalV / 32; i += kLocalThreads) {
+            fwm[i] = 0; bwm[i] = 0; frm[0][i] = 0; frm[1][i] = 0;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) { fwm[0] = 1u; frm[0][0] = 1u; bwm[0] = 1u; s_min = 0x7fffffff; }
+        __syncthreads();
+        for (int lv = 0, fc = 0; lv < kLocalV; ++lv, fc ^= 1) {  // forward, frontier push
+            __syncthreads();  // all threads have read s_flag and frm of the last level
+            if (threadIdx.x == 0) s_flag = 0;
+            for (int i = threadIdx.x; i < kLocalV / 32; i += kLocalThreads) frm[fc ^ 1][i] = 0;
+            __syncthreads();
+            for (int i = threadIdx.x; i < nv; i += kLocalThreads) {
+                if (!((frm[fc][i >> 5] >> (i & 31)) & 1u)) continue;
+                for (int e = loff[i]; e < loff[i + 1]; ++e) {
+                    int w = ladj[e];
+                    uint32_t bb = 1u << (w & 31);
+                    if (!(atomicOr(&fwm[w >> 5], bb) & bb)) {
+                        atomicOr(&frm[fc ^ 1][w >> 5], bb);
+                        s_flag = 1;
+                    }
+                }
+            }
+            __syncthreads();
+            if (!s_flag) break;
+        }
+        for (int lv = 0; lv < kLocalV; ++lv) {  // backward, pull over out-edges
+            __syncthreads();
+            if (threadIdx.x == 0) s_flag = 0;
+            __syncthreads();
+            for (int i = threadIdx.x; i < nv; i += kLocalThreads) {
+                if ((bwm[i >> 5] >> (i & 31)) & 1u) continue;
+                for (int e = loff[i]; e < loff[i + 1]; ++e)
+                    if ((bwm[ladj[e] >> 5] >> (ladj[e] & 31)) & 1u) {
+                        atomicOr(&bwm[i >> 5], 1u << (i & 31));
+                        s_flag = 1;
+                        break;
+                    }
+            }
+            __syncthreads();
+            if (!s_flag) break;
+        }
+        int both = 0;
+        for (int i = threadIdx.x; i < nw; i += kLocalThreads) {
+            uint32_t m = fwm[i] & bwm[i];
+            if (i == nw - 1 && (nv & 31)) m &= (1u << (nv & 31)) - 1u;
+            both += __popc(m);
+        }
+        for (int o = 16; o; o >>= 1) both += __shfl_xor_sync(kFull, both, o);
+        __syncthreads();
+        if (threadIdx.x == 0) s_both = 0;
+        __syncthreads();
+        if (lane_id() == 0) atomicAdd(&s_both, both);
+        for (int i = threadIdx.x; i < nv; i += kLocalThreads) atomicMin(&s_min, gid[i]);
+        __syncthreads();
+        if (s_both == nv) {  // single SCC
+            const int32_t mn = s_min;
+            for (int i = threadIdx.x; i < nv; i += kLocalThreads) {
+                r.label[gid[i]] = mn;
+                r.cls[gid[i]] = CLS_MICE;
+            }
+            if (threadIdx.x == 0) {
+                atomicAdd((unsigned long long *)(r.hist + nv), 1ull);  // nv <= kLocalV
+                atomicAdd(r.counters + C_MICE_SCC, 1ull);
+                atomicAdd(r.counters + C_MICE_V, (unsigned long long)nv);
+                atomicAdd(r.counters + C_LOCAL_WCC, 1ull);
+            }
+        } else if (threadIdx.x == 0) {
             // iterative Tarjan over the local CSR
             for (int i = 0; i < nv; ++i) { idx[i] = -1; onst[i] = 0; }
             int counter = 0, sp = 0, nscc = 0;
@@ -896,15 +1014,26 @@ __global__ void __launch_bounds__(kBlock) k_color(Run<OffT> r, Ext<OffT> x) {
 // here is an internal error.
 template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_finalize(Run<OffT> r, Ext<OffT> x) {
+    constexpr int U = 4;
     const int lane = lane_id();
     const int64_t gw = ((int64_t)blockIdx.x * kBlock + threadIdx.x) >> 5;
     const int64_t nw = (int64_t)gridDim.x * kWarps;
-    for (int64_t wi = gw; wi < r.W; wi += nw) {
-        uint32_t s = r.B[wi];
-        if (r.A[wi] && lane == 0) atomicCAS(r.err, 0, kErrOverflow);
-        if (!s) continue;
-        int64_t v = wi * 32 + lane;
-        if ((s >> lane) & 1u) r.label[v] = r.gmin[seg_of(r.vbase, r.nseg, v)];
+    for (int64_t wb = gw * U; wb < r.W; wb += nw * U) {
+        uint32_t t[U], b[U], a[U];
+#pragma unroll
+        for (int j = 0; j < U; ++j) {
+            const int64_t wi = wb + j;
+            t[j] = wi < r.W ? r.T[wi] : 0u;
+            b[j] = wi < r.W ? r.B[wi] : 0u;
+            a[j] = wi < r.W ? r.A[wi] : 0u;
+        }
+#pragma unroll
+        for (int j = 0; j < U; ++j) {
+            if (a[j] && lane == 0) atomicCAS(r.err, 0, kErrOverflow);  // every vertex must be labelled
+            const int64_t v = (wb + j) * 32 + lane;
+            if ((b[j] >> lane) & 1u) r.label[v] = r.gmin[seg_of(r.vbase, r.nseg, v)];
+            else if ((t[j] >> lane) & 1u) r.label[v] = (int32_t)v;
+        }
     }
     const int64_t gt = (int64_t)blockIdx.x * kBlock + threadIdx.x;
     for (int64_t sg = gt; sg < r.nseg; sg += (int64_t)gridDim.x * kBlock) {
