@@ -112,6 +112,27 @@ int ispan_scc_run(ispan_ctx *ctx, const ispan_csr *g, const ispan_params *p,
 int ispan_scc_run_batch(ispan_ctx *ctx, const ispan_csr *g, int32_t nseg, const int64_t *vbase,
                         const ispan_params *p, int32_t *labels_out, ispan_stats *st);
 
+/* Largest graph (vertices) that ispan_scc_small_noalloc accepts. */
+#define ISPAN_NOALLOC_MAX_V 65536
+
+/* SCC labels of one small graph without allocating any device memory.
+ * No counterpart in the reference.  For callers that cannot call cudaMalloc:
+ * code running under another framework's memory manager (which owns the
+ * device memory), latency-critical paths that cannot take cudaMalloc's
+ * implicit synchronisation, or code issuing work during stream capture.
+ * g must be device-resident (on_device = 1; only the forward CSR is read);
+ * labels_out is device memory of V entries and receives the same canonical
+ * min-id labels as ispan_scc_run.  The work is one kernel launched on
+ * `stream` (NULL: the default stream); the call returns once it is queued.
+ * Scratch is a fixed 2 MiB device array inside the library, so graphs above
+ * ISPAN_NOALLOC_MAX_V vertices are rejected with ISPAN_ERR_CAPACITY.  Every
+ * device that loads the library holds that array until the process exits.
+ * The first call on a device resolves the array's address (no allocation);
+ * make that first call before any stream capture.  All calls on a device
+ * share the one array: calls that overlap on the GPU (different streams,
+ * no ordering between them) race and must not be issued. */
+int ispan_scc_small_noalloc(const ispan_csr *g, int32_t *labels_out, void *stream);
+
 /* Reference-convention per-vertex codes from canonical labels and the class
  * of each vertex, as get_scc_result (src/load_print.cpp:24-60) expects:
  * 1 giant, -1 trimmed size-1, -2 size-2, -3 size-3, otherwise label + 2;

@@ -23,6 +23,7 @@ F_STAGE_TIMES = 4
 F_NO_L2_WINDOW = 8
 F_VALIDATE = 16
 F_EXACT_STATS = 32
+NOALLOC_MAX_V = 65536
 
 
 class IspanError(RuntimeError):
@@ -78,6 +79,7 @@ def lib() -> C.CDLL:
                                           C.POINTER(Stats)]
         L.ispan_ref_codes.argtypes = [P, P]
         L.ispan_debug_trace.argtypes = [P, P, C.c_int64]
+        L.ispan_scc_small_noalloc.argtypes = [C.POINTER(Csr), P, P]
         L.ispan_strerror.argtypes = [C.c_int]
         L.ispan_strerror.restype = C.c_char_p
         L.ispan_version.restype = C.c_char_p
@@ -86,7 +88,8 @@ def lib() -> C.CDLL:
 
 
 SYMBOLS = ("ispan_ctx_create", "ispan_ctx_destroy", "ispan_ctx_set_stream", "ispan_ctx_bytes", "ispan_scc_run",
-           "ispan_scc_run_batch", "ispan_ref_codes", "ispan_debug_trace", "ispan_strerror", "ispan_version")
+           "ispan_scc_run_batch", "ispan_ref_codes", "ispan_debug_trace", "ispan_scc_small_noalloc", "ispan_strerror",
+           "ispan_version")
 
 
 def check(rc: int, what: str = "") -> None:
