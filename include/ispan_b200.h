@@ -141,8 +141,12 @@ int ispan_scc_small_noalloc(const ispan_csr *g, int32_t *labels_out, void *strea
 int ispan_ref_codes(ispan_ctx *ctx, int32_t *codes_out);
 
 /* Diagnostics: per-level trace of the two reachability searches of the last
- * run, [2][256][4] int64 (direction, level): mode (0 top-down, 1 bottom-up,
- * 2 small-frontier tail), vertices reached, frontier edges, %globaltimer ns.
+ * run, [3][256][4] int64: for the forward (0) and backward (1) search, per
+ * level, mode (0 top-down, 1 bottom-up, 2 asynchronous), vertices reached,
+ * frontier edges, %globaltimer ns; for the large-WCC rounds (2), per round,
+ * round number (bits 0-15; grid-wide rounds of its forward search in bits
+ * 16-39, of its backward search from bit 40), vertices left, pivots,
+ * %globaltimer ns.
  * No counterpart in the reference (its VERBOSE "Level-k" lines, src/fw_bw.h:557-572,
  * print the same kind of record). */
 int ispan_debug_trace(ispan_ctx *ctx, int64_t *out, int64_t cap);

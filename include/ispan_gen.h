@@ -64,6 +64,12 @@ int ispan_gen_copy(const ispan_gen_graph *g, void *fw_beg, int32_t *fw_adj, void
 int ispan_gen_device_ptrs(const ispan_gen_graph *g, const int64_t **fw_beg, const int32_t **fw_adj,
                           const int64_t **bw_beg, const int32_t **bw_adj);
 
+/* One graph of a batch, [vlo, vhi) of a disjoint union, with local ids
+ * (minus vlo) into caller device buffers; *E_out gets its edge count (query
+ * first with all array pointers NULL). */
+int ispan_gen_extract(const ispan_gen_graph *g, int64_t vlo, int64_t vhi, void *fw_beg, int32_t *fw_adj,
+                      void *bw_beg, int32_t *bw_adj, int32_t offset_bytes, int64_t *E_out);
+
 int ispan_gen_free(ispan_gen_graph *g);
 
 #ifdef __cplusplus

@@ -133,17 +133,36 @@ class Context:
             stats["histogram"] = {int(s): int(c) for s, c in zip(hs[:n], hc[:n])}
         return labels_out[:V], stats
 
+    def run_raw(self, V, E, fw_beg, fw_adj, bw_beg, bw_adj, offset_bytes, labels_out, vbase=None,
+                alpha=30, beta=200, gamma=10, theta=0.1, stage_times=False, exact_stats=False):
+        """Run on raw device pointers (e.g. a generator's arrays, no copy);
+        labels_out is a CUDA tensor of V int32."""
+        g = _lib.Csr(int(V), int(E), int(fw_beg), int(bw_beg), int(fw_adj), int(bw_adj), int(offset_bytes), 1)
+        flags = _lib.F_LABELS_ON_DEVICE | (_lib.F_STAGE_TIMES if stage_times else 0) | \
+            (_lib.F_EXACT_STATS if exact_stats else 0)
+        p = _lib.Params(alpha, beta, gamma, theta, flags)
+        st = _lib.Stats()
+        L = _lib.lib()
+        if vbase is None:
+            rc = L.ispan_scc_run(self._h, C.byref(g), C.byref(p), C.c_void_p(_ptr(labels_out)), C.byref(st))
+        else:
+            vb = np.ascontiguousarray(vbase, np.int64)
+            rc = L.ispan_scc_run_batch(self._h, C.byref(g), len(vb) - 1, vb.ctypes.data, C.byref(p),
+                                       C.c_void_p(_ptr(labels_out)), C.byref(st))
+        check(rc, "ispan_scc_run")
+        return labels_out, st.as_dict()
+
     def run_csr(self, csr: CSR, **kw):
         return self.run(csr.fw_beg, csr.fw_adj, csr.bw_beg, csr.bw_adj, V=csr.V, **kw)
 
     def trace(self):
-        """Per-level records of the last run's FW and BW searches: lists of
-        (mode, reached, frontier_edges, t_ns) for each direction."""
-        t = np.zeros(2 * 256 * 4, np.int64)
+        """Per-level records of the last run: FW and BW searches (mode, reached,
+        frontier_edges, t_ns) and the large-WCC rounds (round, left, pivots, t_ns)."""
+        t = np.zeros(3 * 256 * 4, np.int64)
         check(_lib.lib().ispan_debug_trace(self._h, t.ctypes.data, len(t)), "ispan_debug_trace")
-        t = t.reshape(2, 256, 4)
+        t = t.reshape(3, 256, 4)
         out = []
-        for d in range(2):
+        for d in range(3):
             rows = [tuple(int(x) for x in r) for r in t[d] if r[3] != 0]
             out.append(rows)
         return out

@@ -290,6 +290,19 @@ __global__ void k_offsets(const uint64_t *k, int64_t n, int64_t V, int64_t *beg,
     }
 }
 
+// offsets of a vertex range [vlo, vlo + vcount) from keys sorted by src:
+// beg_out points at beg[vlo], adj_out at the range's first edge, ebase is the
+// global index of that edge
+__global__ void k_offsets_range(const uint64_t *k, int64_t n, int64_t vlo, int64_t vcount, int64_t *beg_out,
+                                int32_t *adj_out, int64_t ebase) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i <= n; i += (int64_t)gridDim.x * blockDim.x) {
+        int64_t s = i < n ? (int64_t)(k[i] >> 32) - vlo : vcount;
+        int64_t p = i > 0 ? (int64_t)(k[i - 1] >> 32) - vlo : -1;
+        for (int64_t v = p + 1; v <= s && v <= vcount; ++v) beg_out[v] = ebase + i;
+        if (i < n) adj_out[i] = (int32_t)(k[i] & 0xffffffffull);
+    }
+}
+
 __global__ void k_swap(const uint64_t *in, uint64_t *out, int64_t n) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         uint64_t x = in[i];
@@ -343,6 +356,47 @@ static int build_csr(uint64_t *a, uint64_t *b, int64_t n, int64_t V, ispan_gen_g
     cudaFree(tmp);
     cudaFree(flag);
     cudaFree(nsel);
+    return 0;
+}
+
+// Sort a group of keys whose endpoints lie in [vlo, vlo + vcount), drop
+// self-loops and duplicates, and write both CSR directions of that vertex
+// range into the final arrays at edge bases fw_eb / bw_eb.  Returns the
+// group's edge count in *E_out.  a, b: key buffers of n entries.
+static int build_csr_range(uint64_t *a, uint64_t *b, int64_t n, int64_t vlo, int64_t vcount, ispan_gen_graph *g,
+                           int64_t eb, int64_t *E_out) {
+    const int vbits = bits_for(vlo + vcount);
+    const int G = 148 * 8, T = 256;
+    size_t tmp_bytes = 0, t2 = 0;
+    cub::DoubleBuffer<uint64_t> db(a, b);
+    GK(cub::DeviceRadixSort::SortKeys(nullptr, tmp_bytes, db, n, 0, 32 + vbits));
+    uint8_t *flag = nullptr;
+    int64_t *nsel = nullptr;
+    GK(cudaMalloc(&flag, std::max<int64_t>(n, 1)));
+    GK(cudaMalloc(&nsel, sizeof(int64_t)));
+    GK(cub::DeviceSelect::Flagged(nullptr, t2, a, flag, b, nsel, n));
+    void *tmp = nullptr;
+    GK(cudaMalloc(&tmp, std::max(tmp_bytes, t2) + 256));
+    GK(cub::DeviceRadixSort::SortKeys(tmp, tmp_bytes, db, n, 0, 32 + vbits));
+    uint64_t *sorted = db.Current(), *other = db.Alternate();
+    k_flag_unique<<<G, T>>>(sorted, n, flag);
+    GK(cudaGetLastError());
+    GK(cub::DeviceSelect::Flagged(tmp, t2, sorted, flag, other, nsel, n));
+    int64_t E = 0;
+    GK(cudaMemcpy(&E, nsel, sizeof(int64_t), cudaMemcpyDeviceToHost));
+    k_offsets_range<<<G, T>>>(other, E, vlo, vcount, g->fw_beg + vlo, g->fw_adj + eb, eb);
+    GK(cudaGetLastError());
+    k_swap<<<G, T>>>(other, sorted, E);
+    GK(cudaGetLastError());
+    cub::DoubleBuffer<uint64_t> db2(sorted, other);
+    GK(cub::DeviceRadixSort::SortKeys(tmp, tmp_bytes, db2, E, 0, 32 + vbits));
+    k_offsets_range<<<G, T>>>(db2.Current(), E, vlo, vcount, g->bw_beg + vlo, g->bw_adj + eb, eb);
+    GK(cudaGetLastError());
+    GK(cudaDeviceSynchronize());
+    cudaFree(tmp);
+    cudaFree(flag);
+    cudaFree(nsel);
+    *E_out = E;
     return 0;
 }
 
@@ -470,14 +524,17 @@ __global__ void k_web(WebProg P, uint64_t *keys, int64_t total) {
 struct BatchProg {
     uint64_t seed;
     int32_t nseg, max_cycle;
+    int32_t g0;             // first graph of this group
+    int64_t i0;             // first item of this group
     const int64_t *vbase;   // [nseg+1]
     const int64_t *ibase;   // [nseg+1] item prefix
     const int32_t *scale;   // [nseg] R-MAT scale (2^scale >= V_g)
 };
 
 __global__ void k_batch(BatchProg P, uint64_t *keys, int64_t total) {
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
-        int lo = 0, hi = P.nseg - 1;
+    for (int64_t ii = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; ii < total; ii += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = ii + P.i0;
+        int lo = P.g0, hi = P.nseg - 1;
         while (lo < hi) {
             int mid = (lo + hi + 1) >> 1;
             if (P.ibase[mid] <= i) lo = mid; else hi = mid - 1;
@@ -514,7 +571,7 @@ __global__ void k_batch(BatchProg P, uint64_t *keys, int64_t total) {
                 key = ((uint64_t)(vb + x) << 32) | (uint64_t)(vb + y);
             }
         }
-        keys[i] = key;
+        keys[ii] = key;
     }
 }
 
@@ -705,7 +762,7 @@ int ispan_gen_batch(int device, int32_t nseg, int64_t vmin, int64_t vmax, int32_
     }
     if (vb[nseg] >= (1ll << 31) - 1) return -1;
     memcpy(vbase_out, vb.data(), (nseg + 1) * sizeof(int64_t));
-    int64_t total = ib[nseg];
+    const int64_t total = ib[nseg], V = vb[nseg];
     int64_t *d_vb = nullptr, *d_ib = nullptr;
     int32_t *d_sc = nullptr;
     GK(cudaMalloc(&d_vb, vb.size() * 8));
@@ -714,14 +771,45 @@ int ispan_gen_batch(int device, int32_t nseg, int64_t vmin, int64_t vmax, int32_
     GK(cudaMemcpy(d_vb, vb.data(), vb.size() * 8, cudaMemcpyHostToDevice));
     GK(cudaMemcpy(d_ib, ib.data(), ib.size() * 8, cudaMemcpyHostToDevice));
     GK(cudaMemcpy(d_sc, sc.data(), sc.size() * 4, cudaMemcpyHostToDevice));
-    BatchProg P{seed, nseg, max_cycle, d_vb, d_ib, d_sc};
-    uint64_t *ka, *kb;
-    if (alloc_keys(total, &ka, &kb)) return -2;
-    k_batch<<<148 * 16, 256>>>(P, ka, total);
-    GK(cudaGetLastError());
     ispan_gen_graph *g = new ispan_gen_graph();
     g->device = device;
-    int rc = build_csr(ka, kb, total, vb[nseg], g);
+    g->V = V;
+    // final arrays sized for the sampled edges; the CSR of each group of
+    // graphs is built with its keys alone (a group's keys stay under ~1e9),
+    // so the whole batch never needs keys for all edges at once
+    if (cudaMalloc(&g->fw_beg, (V + 1) * sizeof(int64_t)) != cudaSuccess ||
+        cudaMalloc(&g->bw_beg, (V + 1) * sizeof(int64_t)) != cudaSuccess ||
+        cudaMalloc(&g->fw_adj, std::max<int64_t>(total, 1) * sizeof(int32_t)) != cudaSuccess ||
+        cudaMalloc(&g->bw_adj, std::max<int64_t>(total, 1) * sizeof(int32_t)) != cudaSuccess) {
+        cudaGetLastError();
+        ispan_gen_free(g);
+        return -2;
+    }
+    const int64_t kGroupItems = 1000000000ll;
+    int64_t gmax = 0;
+    for (int g0 = 0; g0 < nseg;) {
+        int g1 = g0 + 1;
+        while (g1 < nseg && ib[g1 + 1] - ib[g0] <= kGroupItems) ++g1;
+        gmax = std::max(gmax, ib[g1] - ib[g0]);
+        g0 = g1;
+    }
+    uint64_t *ka, *kb;
+    if (alloc_keys(gmax, &ka, &kb)) { ispan_gen_free(g); return -2; }
+    int64_t E = 0;
+    int rc = 0;
+    for (int g0 = 0; g0 < nseg && !rc;) {
+        int g1 = g0 + 1;
+        while (g1 < nseg && ib[g1 + 1] - ib[g0] <= kGroupItems) ++g1;
+        BatchProg P{seed, nseg, max_cycle, g0, ib[g0], d_vb, d_ib, d_sc};
+        int64_t n = ib[g1] - ib[g0];
+        k_batch<<<148 * 16, 256>>>(P, ka, n);
+        if (cudaGetLastError() != cudaSuccess) { rc = -3; break; }
+        int64_t Eg = 0;
+        rc = build_csr_range(ka, kb, n, vb[g0], vb[g1] - vb[g0], g, E, &Eg);
+        E += Eg;
+        g0 = g1;
+    }
+    g->E = E;
     cudaFree(ka);
     cudaFree(kb);
     cudaFree(d_vb);
@@ -777,6 +865,39 @@ int ispan_gen_device_ptrs(const ispan_gen_graph *g, const int64_t **fw_beg, cons
     if (fw_adj) *fw_adj = g->fw_adj;
     if (bw_beg) *bw_beg = g->bw_beg;
     if (bw_adj) *bw_adj = g->bw_adj;
+    return 0;
+}
+
+__global__ void k_extract_beg(const int64_t *beg, int64_t vlo, int64_t n, void *out, int ob) {
+    const int64_t b0 = beg[vlo];
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i <= n; i += (int64_t)gridDim.x * blockDim.x) {
+        int64_t x = beg[vlo + i] - b0;
+        if (ob == 8) ((int64_t *)out)[i] = x; else ((int32_t *)out)[i] = (int32_t)x;
+    }
+}
+__global__ void k_extract_adj(const int32_t *adj, int64_t e0, int64_t n, int64_t vlo, int32_t *out) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = (int32_t)(adj[e0 + i] - vlo);
+}
+
+int ispan_gen_extract(const ispan_gen_graph *g, int64_t vlo, int64_t vhi, void *fw_beg, int32_t *fw_adj,
+                      void *bw_beg, int32_t *bw_adj, int32_t offset_bytes, int64_t *E_out) {
+    if (!g || vlo < 0 || vhi > g->V || vhi < vlo || (offset_bytes != 4 && offset_bytes != 8)) return -1;
+    if (cudaSetDevice(g->device) != cudaSuccess) return -3;
+    int64_t f0, f1, b0, b1;
+    GK(cudaMemcpy(&f0, g->fw_beg + vlo, 8, cudaMemcpyDeviceToHost));
+    GK(cudaMemcpy(&f1, g->fw_beg + vhi, 8, cudaMemcpyDeviceToHost));
+    GK(cudaMemcpy(&b0, g->bw_beg + vlo, 8, cudaMemcpyDeviceToHost));
+    GK(cudaMemcpy(&b1, g->bw_beg + vhi, 8, cudaMemcpyDeviceToHost));
+    if (f1 - f0 != b1 - b0) return -1;  // the range is not closed under edges
+    if (E_out) *E_out = f1 - f0;
+    const int64_t n = vhi - vlo;
+    if (fw_beg) k_extract_beg<<<148, 256>>>(g->fw_beg, vlo, n, fw_beg, offset_bytes);
+    if (bw_beg) k_extract_beg<<<148, 256>>>(g->bw_beg, vlo, n, bw_beg, offset_bytes);
+    if (fw_adj) k_extract_adj<<<148 * 4, 256>>>(g->fw_adj, f0, f1 - f0, vlo, fw_adj);
+    if (bw_adj) k_extract_adj<<<148 * 4, 256>>>(g->bw_adj, b0, b1 - b0, vlo, bw_adj);
+    GK(cudaGetLastError());
+    GK(cudaDeviceSynchronize());
     return 0;
 }
 

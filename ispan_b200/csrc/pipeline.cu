@@ -171,7 +171,7 @@ static int ctx_alloc(ispan_ctx *c) {
     rc |= dalloc(&c->gsync, 4, o);
     rc |= dalloc(&c->err, 4, o);
     rc |= dalloc(&c->bfsctl, 1, o);
-    rc |= dalloc(&c->trace, 2 * kTraceLevels * 4, o);
+    rc |= dalloc(&c->trace, 3 * kTraceLevels * 4, o);
     return rc ? ISPAN_ERR_NOMEM : ISPAN_OK;
 }
 
@@ -282,7 +282,7 @@ static cudaError_t enqueue(ispan_ctx *c, Run<OffT> r, Ext<OffT> x, bool times, b
     if ((e = cudaMemsetAsync(c->hist, 0, (kHistCap + kBigCap) * sizeof(int64_t), s))) return e;
     if ((e = cudaMemsetAsync(c->gsync, 0, 4 * sizeof(unsigned), s))) return e;
     if ((e = cudaMemsetAsync(c->err, 0, 4 * sizeof(int), s))) return e;
-    if ((e = cudaMemsetAsync(c->trace, 0, 2 * kTraceLevels * 4 * sizeof(long long), s))) return e;
+    if ((e = cudaMemsetAsync(c->trace, 0, 3 * kTraceLevels * 4 * sizeof(long long), s))) return e;
     if ((e = cudaMemsetAsync(c->pivot_key, 0, r.nseg * sizeof(unsigned long long), s))) return e;
     if ((e = cudaMemsetAsync(c->gsize, 0, r.nseg * sizeof(unsigned long long), s))) return e;
     if ((e = cudaMemsetAsync(c->gmin, 0x7f, r.nseg * sizeof(int32_t), s))) return e;
@@ -718,7 +718,7 @@ int ispan_ref_codes(ispan_ctx *c, int32_t *codes) {
 int ispan_debug_trace(ispan_ctx *c, int64_t *out, int64_t cap) {
     if (!c || !out) return ISPAN_ERR_ARG;
     std::lock_guard<std::mutex> lock(c->mu);
-    int64_t n = std::min<int64_t>(cap, 2 * kTraceLevels * 4);
+    int64_t n = std::min<int64_t>(cap, 3 * kTraceLevels * 4);
     CK(cudaMemcpy(out, c->trace, n * sizeof(int64_t), cudaMemcpyDeviceToHost));
     return ISPAN_OK;
 }

@@ -20,7 +20,7 @@ enum Cls : uint8_t { CLS_NONE = 0, CLS_GIANT = 1, CLS_TRIM1 = 2, CLS_TRIM2 = 3, 
 // control-block slots (Run::ctl64): worklist and queue counters
 enum Ctl64 {
     K_WL0 = 0, K_WL1, K_CQ0, K_CQ1, K_CQ2, K_ROOTS, K_SMALL, K_LARGE, K_ALLOC, K_LARGE2,
-    K_SPILL, K_MICE_SCC, K_LOCAL_NEXT, kNumCtl = 32
+    K_SPILL, K_MICE_SCC, K_LOCAL_NEXT, K_MINPRIO0, K_MINPRIO1, kNumCtl = 32
 };
 
 constexpr int kLocalV = 1024;   // a WCC up to this many vertices ...
@@ -146,16 +146,19 @@ __global__ void __launch_bounds__(kBlock) k_trim1_first(Run<OffT> r, Ext<OffT> x
             }
             if (r.nseg == 1) {
                 best = key > best ? key : best;
-            } else {
-                // segmented: lanes of one word nearly always share a graph
-                int sg = valid[j] ? seg_of(r.vbase, r.nseg, v) : -1;
-                int s0 = __shfl_sync(kFull, sg, 0);
-                bool uni = __all_sync(kFull, sg == s0 || sg < 0);
-                if (uni) {
+            } else if (__any_sync(kFull, key != 0)) {
+                // segmented: graphs are contiguous id ranges, so the word's first
+                // and last vertex decide whether all lanes share one graph
+                const int64_t vl = min(wi * 32 + 31, r.V - 1);
+                int s0 = 0, s1 = 0;
+                if (lane == 0) { s0 = seg_of(r.vbase, r.nseg, wi * 32); s1 = seg_of(r.vbase, r.nseg, vl); }
+                s0 = __shfl_sync(kFull, s0, 0);
+                s1 = __shfl_sync(kFull, s1, 0);
+                if (s0 == s1) {
                     unsigned long long m = warp_max_u64(key);
                     if (lane == 0 && m) atomicMax(r.pivot_key + s0, m);
                 } else if (key) {
-                    atomicMax(r.pivot_key + sg, key);
+                    atomicMax(r.pivot_key + seg_of(r.vbase, r.nseg, v), key);
                 }
             }
         }
@@ -229,13 +232,20 @@ __global__ void __launch_bounds__(kBlock) k_giant_residual(Run<OffT> r, Ext<OffT
             if (r.nseg == 1) {
                 gm = min(gm, v0);
             } else {
-                for (uint32_t m = b; m;) {  // members may span graphs
-                    int bit = __ffs(m) - 1;
-                    int64_t v = wi * 32 + bit;
-                    int sg = seg_of(r.vbase, r.nseg, v);
-                    atomicMin(r.gmin + sg, (int)v);
-                    atomicAdd(r.gsize + sg, 1ull);
-                    m &= m - 1;
+                const int64_t vlast = wi * 32 + 31 - __clz(b);
+                const int sa = seg_of(r.vbase, r.nseg, v0), sb = seg_of(r.vbase, r.nseg, vlast);
+                if (sa == sb) {  // graphs are contiguous ranges: one graph holds the whole word
+                    atomicMin(r.gmin + sa, v0);
+                    atomicAdd(r.gsize + sa, (unsigned long long)__popc(b));
+                } else {
+                    for (uint32_t m = b; m;) {  // the word straddles graphs
+                        int bit = __ffs(m) - 1;
+                        int64_t v = wi * 32 + bit;
+                        int sg = seg_of(r.vbase, r.nseg, v);
+                        atomicMin(r.gmin + sg, (int)v);
+                        atomicAdd(r.gsize + sg, 1ull);
+                        m &= m - 1;
+                    }
                 }
             }
         }
@@ -840,144 +850,294 @@ __global__ void __launch_bounds__(kLocalThreads) k_local_scc(Run<OffT> r, Ext<Of
 }
 
 // ---------------------------------------------------------------------------
-// Large WCCs: colouring rounds (the reference's dead color_propagation /
-// color_identify, src/color_propagation.h:64-466, restated as the pipeline's
-// mice stage).  Per round: every active vertex starts with its own id as
-// colour; colours relax to the minimum over all forward ancestors with a
-// frontier-driven propagation; a vertex whose colour is its own id is a root;
-// a backward search from all roots at once, restricted to the root's colour,
-// collects exactly the root's SCC (all ancestors of a member reach the root,
-// so the member's colour is the root's id; the root is the SCC's minimum
-// vertex, i.e. its canonical label).  Found SCCs leave; the rest recolour.
+// Large WCCs: colouring rounds inside classes (the reference's dead
+// color_propagation / color_identify, src/color_propagation.h:64-466, made
+// the mice stage; it replaces the serial per-pivot mice_fw_bw,
+// src/fw_bw.h:1585-1691).
+//
+// Every active vertex has a priority -- a bijective hash of its id, so
+// priorities are random with respect to the graph -- and a class (initially
+// its WCC).  Each round a sample of the vertices are pivots: those whose
+// priority lies below a threshold that doubles every round (about 1024
+// pivots in the first round, every vertex after log2(n/1024) rounds), plus
+// the residual's minimum-priority vertex.  A pivot's colour starts as its
+// priority, every other colour as "none", and colours relax to the minimum
+// over the forward ancestors *inside the class*.  A pivot whose colour is its
+// own priority is a root; a backward search from all roots at once,
+// restricted to the root's colour, collects exactly the root's SCC (every
+// ancestor of a member reaches the root, so it has the root's colour).  The
+// SCC takes its minimum member id as label and leaves.  Every SCC lies in a
+// single colour, so the colour groups of a round (and the vertices no pivot
+// reached) are independent sub-problems: a reached vertex's colour becomes
+// its class for the next round, an unreached one keeps its class.
+//
+// Round count and work: with one pivot per class this is forward-backward
+// (one SCC per class per round: 108 rounds on the batch workload); with
+// every vertex a pivot it is colouring, O(log n) rounds like a treap but each
+// vertex's colour drops about ln(#ancestors) times, each drop re-pushing its
+// out-edges (10x the work per round).  A sample that grows from small keeps
+// the drops per vertex near ln(#pivot ancestors) while classes are large and
+// reaches full colouring only once classes are small.
+//
+// Both searches run as asynchronous rounds: each CTA takes a slice of the
+// global frontier and works it to exhaustion with a frontier in shared
+// memory (levels separated by __syncthreads), overflowing to the global
+// queue; a grid barrier separates rounds, so ring-shaped SCCs cost no grid
+// barrier per hop.
+__device__ __forceinline__ uint32_t prio_of(uint32_t v) {
+    // bijection on 32 bits: xor-shifts and odd multipliers are invertible
+    v ^= v >> 16;
+    v *= 0x7feb352du;
+    v ^= v >> 15;
+    v *= 0x846ca68bu;
+    v ^= v >> 16;
+    return v;
+}
+
+constexpr int kCLQ = 2048;
+struct ColorSmem {
+    int32_t lq[2][kCLQ];
+    int cnt[2];
+};
+
+// One asynchronous round over the global queue q_in[0..n_in).  KIND 0
+// relaxes colours forward inside the class (push the smaller colour to
+// out-neighbours of the same class, re-queueing them); KIND 1 grows each
+// root's SCC backward inside its colour (claim in-neighbours in F).
+template <typename OffT, int KIND>
+__device__ __forceinline__ void color_async_round(const Run<OffT> &r, const Ext<OffT> &x, const int32_t *q_in,
+                                                  int64_t n_in, int32_t *q_out, unsigned long long *n_out,
+                                                  ColorSmem &sm) {
+    uint32_t *col = reinterpret_cast<uint32_t *>(r.parent);
+    const uint32_t *cls = reinterpret_cast<const uint32_t *>(r.qe[0]);
+    int32_t *rootof = r.aux2;
+    const OffT *beg = KIND == 0 ? r.fw_beg : r.bw_beg;
+    const int32_t *adj = KIND == 0 ? r.fw_adj : r.bw_adj;
+    const int tid = threadIdx.x;
+    const int64_t s0 = n_in * blockIdx.x / gridDim.x, s1 = n_in * (blockIdx.x + 1) / gridDim.x;
+    for (int64_t bs = s0; bs < s1; bs += kCLQ) {
+        const int n0 = (int)min((int64_t)kCLQ, s1 - bs);
+        __syncthreads();
+        for (int i = tid; i < n0; i += kBlock) sm.lq[0][i] = __ldcg(q_in + bs + i);
+        if (tid == 0) { sm.cnt[0] = n0; sm.cnt[1] = 0; }
+        __syncthreads();
+        int c = 0;
+        for (int it = 0; it < (1 << 20); ++it) {
+            const int n = sm.cnt[c];
+            if (n == 0) break;
+            for (int i = tid; i < n; i += kBlock) {
+                const int32_t v = sm.lq[c][i];
+                uint32_t cv;
+                if (KIND == 0) {
+                    clear_bit(r.D, v);
+                    __threadfence();  // clear the queued mark before reading the colour
+                }
+                cv = __ldcg(col + v);
+                const uint32_t kv = __ldcg(cls + v);
+                const int32_t rt = KIND == 1 ? __ldcg(rootof + v) : 0;
+                const int64_t e0 = ld_off(beg, v), e1 = ld_off(beg, v + 1);
+                for (int64_t e = e0; e < e1; e += 4) {
+                    int32_t w[4];
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) w[q] = e + q < e1 ? ld_adj(adj, e + q) : -1;
+                    bool ok[4];
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        ok[q] = w[q] >= 0 && w[q] != v && bitv(r.A, w[q]);
+                        if (ok[q]) ok[q] = __ldcg(cls + w[q]) == kv;
+                        if (ok[q]) ok[q] = KIND == 0 ? cv < __ldcg(col + w[q])
+                                                     : (__ldcg(col + w[q]) == cv && !bitv(r.F, w[q]));
+                    }
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        if (!ok[q]) continue;
+                        if (KIND == 0) {
+                            if (cv >= atomicMin(col + w[q], cv)) continue;
+                            __threadfence();  // the new colour is visible before the mark test
+                            if (!set_bit(r.D, w[q])) continue;  // already queued
+                        } else {
+                            if (!set_bit(r.F, w[q])) continue;
+                            rootof[w[q]] = rt;
+                        }
+                        const int pos = atomicAdd(&sm.cnt[c ^ 1], 1);
+                        if (pos < kCLQ) {
+                            sm.lq[c ^ 1][pos] = w[q];
+                        } else {
+                            unsigned long long gp = atomicAdd(n_out, 1ull);
+                            if (VOK((long long)gp, 18)) q_out[gp] = w[q];
+                        }
+                    }
+                }
+            }
+            __syncthreads();
+            if (tid == 0) {
+                sm.cnt[c ^ 1] = min(sm.cnt[c ^ 1], kCLQ);
+                sm.cnt[c] = 0;
+            }
+            __syncthreads();
+            c ^= 1;
+        }
+    }
+}
+
+// Asynchronous rounds until the global queue is empty.  Round 0 reads
+// (q0, n0); later rounds alternate between the two cascade queues with three
+// rotating counters.  Returns the number of rounds, or -1 if a grid barrier
+// failed.
+template <typename OffT, int KIND>
+__device__ __forceinline__ int color_async(const Run<OffT> &r, const Ext<OffT> &x, const int32_t *q0, int64_t n0,
+                                           unsigned long long *cqc, ColorSmem &sm) {
+    for (int lv = 0; lv < (1 << 30); ++lv) {
+        const int64_t n = lv == 0 ? n0 : (int64_t)__ldcg(cqc + lv % 3);
+        if (n == 0) return lv;
+        if (blockIdx.x == 0 && threadIdx.x == 0) cqc[(lv + 2) % 3] = 0ull;
+        const int32_t *q = lv == 0 ? q0 : x.cq[lv & 1];
+        color_async_round<OffT, KIND>(r, x, q, n, x.cq[(lv + 1) & 1], cqc + (lv + 1) % 3, sm);
+        if (!grid_sync(r.gsync, r.err)) return -1;
+        if (lv > 64 * (r.V + 2)) {  // colours only decrease; more rounds is a bug
+            if (threadIdx.x == 0) atomicCAS(r.err, 0, kErrOverflow);
+            return -1;
+        }
+    }
+    return -1;
+}
+
 template <typename OffT>
-__global__ void __launch_bounds__(kBlock) k_color(Run<OffT> r, Ext<OffT> x) {
+__global__ void __launch_bounds__(kBlock, 1) k_color(Run<OffT> r, Ext<OffT> x) {
     __shared__ int64_t sh[kWarps];
+    __shared__ ColorSmem sm;
     const int64_t gt = (int64_t)blockIdx.x * kBlock + threadIdx.x;
     const int64_t nt = (int64_t)gridDim.x * kBlock;
-    int32_t *col = r.parent;
+    uint32_t *col = reinterpret_cast<uint32_t *>(r.parent);
+    uint32_t *cls = reinterpret_cast<uint32_t *>(r.qe[0]);  // class of each vertex
+    int32_t *rootof = r.aux2;  // root of the SCC a marked vertex belongs to
+    int32_t *mn = r.aux;       // at roots: minimum member id, then the member count
     unsigned long long *cqc = x.ctl + K_CQ0;
-    int cur = 0;
-    int rounds = 0;
+    int cur = 0, rounds = 0;
     int64_t prev_n = INT64_MAX;
+    int shift0 = 0;  // first round: pivots are the priorities below 2^(32 - shift0)
+    {   // initial classes: the WCCs (parent holds the WCC root until colours overwrite it)
+        const int64_t n = (int64_t)__ldcg(x.ctl + K_LARGE);
+        while (shift0 < 31 && (n >> (shift0 + 1)) >= 1024) ++shift0;
+        if (blockIdx.x == 0 && threadIdx.x == 0) x.ctl[K_MINPRIO0] = ~0ull;
+        if (!grid_sync(r.gsync, r.err)) return;
+        uint32_t pm = 0xffffffffu;
+        for (int64_t i = gt; i < n; i += nt) {
+            int32_t v = x.large[0][i];
+            cls[v] = (uint32_t)r.parent[v];
+            pm = min(pm, prio_of((uint32_t)v));
+        }
+        pm = __reduce_min_sync(0xffffffffu, pm);
+        if ((threadIdx.x & 31) == 0) atomicMin(x.ctl + K_MINPRIO0, (unsigned long long)pm);
+        if (!grid_sync(r.gsync, r.err)) return;
+    }
     for (int guard = 0; guard < (1 << 30); ++guard) {
         const int64_t n = (int64_t)__ldcg(x.ctl + (cur == 0 ? K_LARGE : K_LARGE2));
         if (n == 0) break;
-        if (n >= prev_n) {  // every round labels at least the minimum vertex's SCC
+        if (n >= prev_n) {  // every round labels the SCC of each class's lowest priority
             if (threadIdx.x == 0) atomicCAS(r.err, 0, kErrOverflow);
             return;
         }
         prev_n = n;
         ++rounds;
         const int32_t *L = x.large[cur];
+        // pivots: priority below the round's threshold, or the residual's minimum
+        const int shift = max(0, shift0 - (rounds - 1));
+        const unsigned long long thr = 1ull << (32 - shift);
+        const unsigned long long minp = __ldcg(x.ctl + K_MINPRIO0 + cur);
+        unsigned long long *next_minp = x.ctl + K_MINPRIO0 + (cur ^ 1);
         if (blockIdx.x == 0 && threadIdx.x == 0) {
             cqc[0] = 0; cqc[1] = 0; cqc[2] = 0;
             x.ctl[cur == 0 ? K_LARGE2 : K_LARGE] = 0;
         }
-        for (int64_t i = gt; i < n; i += nt) {
-            int32_t v = L[i];
-            col[v] = v;
-            r.aux[v] = 0;       // SCC size at roots
-            clear_bit(r.F, v);  // F: SCC mark of this round
-            clear_bit(r.D, v);  // D: queued-this-level mark
+        if (!grid_sync(r.gsync, r.err)) return;
+        if (blockIdx.x == 0 && threadIdx.x == 0) *next_minp = ~0ull;  // read above, before the barrier
+        for (int64_t i = gt; i - threadIdx.x < n; i += nt) {
+            bool piv = false;
+            int32_t v = 0;
+            if (i < n) {
+                v = L[i];
+                const uint32_t p = prio_of((uint32_t)v);
+                piv = p < thr || p <= minp;
+                col[v] = piv ? p : 0xffffffffu;
+                clear_bit(r.F, v);  // F: SCC mark of this round
+                if (piv) set_bit(r.D, v); else clear_bit(r.D, v);  // D: queued mark
+            }
+            wl_append(piv, v, x.cq[0], cqc + 0);
         }
         if (!grid_sync(r.gsync, r.err)) return;
-        // forward min-colour propagation: level 0 queue = L itself
-        int lv = 0;
-        for (int g2 = 0; g2 < (1 << 30); ++g2) {
-            const int64_t m = lv == 0 ? n : (int64_t)__ldcg(cqc + lv % 3);
-            if (m == 0) break;
-            if (blockIdx.x == 0 && threadIdx.x == 0) cqc[(lv + 2) % 3] = 0ull;
-            const int32_t *q = lv == 0 ? L : x.cq[lv & 1];
-            int32_t *qn = x.cq[(lv + 1) & 1];
-            for (int64_t i = gt; i - threadIdx.x < m; i += nt) {
-                bool live = i < m;
-                int32_t v = live ? __ldcg(q + i) : 0;
-                if (live && lv > 0) {
-                    clear_bit(r.D, v);
-                    __threadfence();  // clear the queued mark before reading the colour
-                }
-                int32_t c = live ? __ldcg(col + v) : 0;
-                int64_t e0 = live ? ld_off(r.fw_beg, v) : 0, e1 = live ? ld_off(r.fw_beg, v + 1) : 0;
-                int64_t len = e1 - e0, maxlen = len;
-                for (int o = 16; o; o >>= 1) maxlen = max(maxlen, __shfl_xor_sync(kFull, maxlen, o));
-                for (int64_t k = 0; k < maxlen; ++k) {
-                    bool push = false;
-                    int32_t w = 0;
-                    if (k < len) {
-                        w = ld_adj(r.fw_adj, e0 + k);
-                        if (w != v && bitv(r.A, w) && c < __ldcg(col + w)) {
-                            int32_t old = atomicMin(col + w, c);
-                            if (c < old) {
-                                __threadfence();  // the new colour is visible before the mark test
-                                push = set_bit(r.D, w);
-                            }
-                        }
-                    }
-                    wl_append(push, w, qn, cqc + (lv + 1) % 3);
-                }
-            }
-            if (!grid_sync(r.gsync, r.err)) return;
-            ++lv;
-        }
-        // backward search from the roots inside each colour
+        // forward min-colour relaxation from the pivots; cqc[0] is freed by
+        // color_async only after every CTA has read it here
+        const int64_t npiv = (int64_t)__ldcg(cqc + 0);
+        const int fw_rounds = color_async<OffT, 0>(r, x, x.cq[0], npiv, cqc, sm);
+        if (fw_rounds < 0) return;
         if (blockIdx.x == 0 && threadIdx.x == 0) { cqc[0] = 0; cqc[1] = 0; cqc[2] = 0; }
         if (!grid_sync(r.gsync, r.err)) return;
-        for (int64_t i = gt; i - threadIdx.x < n; i += nt) {
+        for (int64_t i = gt; i - threadIdx.x < n; i += nt) {  // roots
             bool rt = false;
             int32_t v = 0;
             if (i < n) {
                 v = L[i];
-                rt = __ldcg(col + v) == v;
-                if (rt) set_bit(r.F, v);
+                const uint32_t p = prio_of((uint32_t)v);
+                // colours are pivot priorities, so a match means v is a pivot
+                // unless v's priority is the "none" value itself
+                rt = __ldcg(col + v) == p && (p < thr || p <= minp);
+                if (rt) {
+                    set_bit(r.F, v);
+                    rootof[v] = v;
+                    mn[v] = v;
+                }
             }
             wl_append(rt, v, x.cq[0], cqc + 0);
         }
         if (!grid_sync(r.gsync, r.err)) return;
-        lv = 0;
-        for (int g2 = 0; g2 < (1 << 30); ++g2) {
-            const int64_t m = (int64_t)__ldcg(cqc + lv % 3);
-            if (m == 0) break;
-            if (blockIdx.x == 0 && threadIdx.x == 0) cqc[(lv + 2) % 3] = 0ull;
-            const int32_t *q = x.cq[lv & 1];
-            int32_t *qn = x.cq[(lv + 1) & 1];
-            for (int64_t i = gt; i - threadIdx.x < m; i += nt) {
-                bool live = i < m;
-                int32_t v = live ? __ldcg(q + i) : 0;
-                int32_t c = live ? __ldcg(col + v) : 0;
-                int64_t e0 = live ? ld_off(r.bw_beg, v) : 0, e1 = live ? ld_off(r.bw_beg, v + 1) : 0;
-                int64_t len = e1 - e0, maxlen = len;
-                for (int o = 16; o; o >>= 1) maxlen = max(maxlen, __shfl_xor_sync(kFull, maxlen, o));
-                for (int64_t k = 0; k < maxlen; ++k) {
-                    bool push = false;
-                    int32_t u = 0;
-                    if (k < len) {
-                        u = ld_adj(r.bw_adj, e0 + k);
-                        if (u != v && bitv(r.A, u) && __ldcg(col + u) == c && !bitv(r.F, u)) push = set_bit(r.F, u);
-                    }
-                    wl_append(push, u, qn, cqc + (lv + 1) % 3);
-                }
-            }
-            if (!grid_sync(r.gsync, r.err)) return;
-            ++lv;
+        // the roots' count stays in cqc[0] until color_async frees that slot
+        // two rounds later, long after every CTA has read it here
+        const int bw_rounds = color_async<OffT, 1>(r, x, x.cq[0], (int64_t)__ldcg(cqc + 0), cqc, sm);
+        if (bw_rounds < 0) return;
+        if (blockIdx.x == 0 && threadIdx.x == 0 && rounds <= kTraceLevels) {  // diagnostics
+            long long *t = r.trace + ((long long)2 * kTraceLevels + rounds - 1) * 4;
+            t[0] = rounds | ((long long)fw_rounds << 16) | ((long long)bw_rounds << 40);
+            t[1] = n;
+            t[2] = npiv;
+            t[3] = (long long)globaltimer();
         }
-        // label the found SCCs, keep the rest for the next round
+        for (int64_t i = gt; i < n; i += nt) {  // minimum member id per SCC
+            int32_t v = L[i];
+            if (bitv(r.F, v)) atomicMin(mn + __ldcg(rootof + v), v);
+        }
+        if (!grid_sync(r.gsync, r.err)) return;
         int64_t nl = 0;
-        for (int64_t i = gt; i - threadIdx.x < n; i += nt) {
+        uint32_t pm = 0xffffffffu;
+        for (int64_t i = gt; i - threadIdx.x < n; i += nt) {  // labels; the rest continues
             bool keep = false;
             int32_t v = 0;
             if (i < n) {
                 v = L[i];
                 if (bitv(r.F, v)) {
-                    int32_t c = __ldcg(col + v);
-                    r.label[v] = c;
+                    r.label[v] = __ldcg(mn + __ldcg(rootof + v));
                     r.cls[v] = CLS_MICE;
-                    atomicAdd(r.aux + c, 1);
                     ++nl;
                 } else {
                     keep = true;
+                    const uint32_t c = __ldcg(col + v);
+                    if (c != 0xffffffffu) cls[v] = c;  // reached: its colour is its next class
+                    pm = min(pm, prio_of((uint32_t)v));
                 }
             }
             wl_append(keep, v, x.large[cur ^ 1], x.ctl + (cur == 0 ? K_LARGE2 : K_LARGE));
+        }
+        pm = __reduce_min_sync(0xffffffffu, pm);
+        if ((threadIdx.x & 31) == 0 && pm != 0xffffffffu) atomicMin(next_minp, (unsigned long long)pm);
+        if (!grid_sync(r.gsync, r.err)) return;
+        for (int64_t i = gt; i < n; i += nt) {  // sizes: reuse mn at the roots
+            int32_t v = L[i];
+            if (bitv(r.F, v) && __ldcg(rootof + v) == v) mn[v] = 0;
+        }
+        if (!grid_sync(r.gsync, r.err)) return;
+        for (int64_t i = gt; i < n; i += nt) {
+            int32_t v = L[i];
+            if (bitv(r.F, v)) atomicAdd(mn + __ldcg(rootof + v), 1);
         }
         if (!grid_sync(r.gsync, r.err)) return;
         int64_t nroots = 0;
@@ -985,8 +1145,8 @@ __global__ void __launch_bounds__(kBlock) k_color(Run<OffT> r, Ext<OffT> x) {
             int32_t v = L[i];
             if (bitv(r.F, v)) {
                 clear_bit(r.A, v);
-                if (__ldcg(col + v) == v) {
-                    int32_t sz = __ldcg(r.aux + v);
+                if (__ldcg(rootof + v) == v) {
+                    int32_t sz = __ldcg(mn + v);
                     if (sz < kHistCap) {
                         atomicAdd((unsigned long long *)(r.hist + sz), 1ull);
                     } else {
@@ -1031,7 +1191,22 @@ __global__ void __launch_bounds__(kBlock) k_finalize(Run<OffT> r, Ext<OffT> x) {
         for (int j = 0; j < U; ++j) {
             if (a[j] && lane == 0) atomicCAS(r.err, 0, kErrOverflow);  // every vertex must be labelled
             const int64_t v = (wb + j) * 32 + lane;
-            if ((b[j] >> lane) & 1u) r.label[v] = r.gmin[seg_of(r.vbase, r.nseg, v)];
+            int32_t gm = 0;
+            if (b[j]) {  // one graph per word unless it straddles a boundary
+                if (r.nseg == 1) {
+                    gm = r.gmin[0];
+                } else {
+                    int s0 = 0, s1 = 0;
+                    if (lane == 0) {
+                        s0 = seg_of(r.vbase, r.nseg, (wb + j) * 32);
+                        s1 = seg_of(r.vbase, r.nseg, min((wb + j) * 32 + 31, r.V - 1));
+                    }
+                    s0 = __shfl_sync(kFull, s0, 0);
+                    s1 = __shfl_sync(kFull, s1, 0);
+                    gm = r.gmin[s0 == s1 ? s0 : seg_of(r.vbase, r.nseg, v)];
+                }
+            }
+            if ((b[j] >> lane) & 1u) r.label[v] = gm;
             else if ((t[j] >> lane) & 1u) r.label[v] = (int32_t)v;
         }
     }

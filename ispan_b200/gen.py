@@ -35,6 +35,7 @@ def lib():
         L.ispan_gen_copy.argtypes = [P, P, P, P, P, I32, I32]
         L.ispan_gen_device_ptrs.argtypes = [P, C.POINTER(P), C.POINTER(P), C.POINTER(P), C.POINTER(P)]
         L.ispan_gen_free.argtypes = [P]
+        L.ispan_gen_extract.argtypes = [P, I64, I64, P, P, P, P, I32, C.POINTER(I64)]
         _lib = L
     return _lib
 
@@ -76,6 +77,26 @@ class DeviceGraph:
         if rc:
             raise RuntimeError(f"ispan_gen_copy failed ({rc})")
         return fb, fa[:self.E], bb, ba[:self.E]
+
+    def extract(self, i, offset_dtype="int32"):
+        """Graph i of a batch as CUDA tensors with local ids."""
+        import torch
+        lo, hi = int(self.vbase[i]), int(self.vbase[i + 1])
+        E = C.c_int64()
+        rc = lib().ispan_gen_extract(self._h, lo, hi, None, None, None, None, 8, C.byref(E))
+        if rc:
+            raise RuntimeError(f"ispan_gen_extract failed ({rc})")
+        dt = getattr(torch, offset_dtype)
+        n, e = hi - lo, E.value
+        fb = torch.empty(n + 1, dtype=dt, device="cuda")
+        bb = torch.empty(n + 1, dtype=dt, device="cuda")
+        fa = torch.empty(max(e, 1), dtype=torch.int32, device="cuda")
+        ba = torch.empty(max(e, 1), dtype=torch.int32, device="cuda")
+        rc = lib().ispan_gen_extract(self._h, lo, hi, fb.data_ptr(), fa.data_ptr(), bb.data_ptr(), ba.data_ptr(),
+                                     fb.element_size(), C.byref(E))
+        if rc:
+            raise RuntimeError(f"ispan_gen_extract failed ({rc})")
+        return fb, fa[:e], bb, ba[:e]
 
     def free(self):
         if self._h:
