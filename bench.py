@@ -407,7 +407,9 @@ def main():
         ("k_bfs<int64,1> (backward reach)", bw_b, bw_ms)
     peak, peak_kind = measured_peak()
     achieved = by / (kms / 1e3) / 1e9
-    traffic = traffic_from_profiles("k_bfs_fw" if "0>" in kern else "k_bfs_bw")
+    # DRAM bytes per launch from the committed ncu capture (social workload only)
+    traffic = traffic_from_profiles("k_bfs_fw" if "0>" in kern else "k_bfs_bw") \
+        if args.workload == "social" and args.scale == 1.0 else None
     roof = {"bound": "hbm", "kernel": kern, "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
             "alg_bytes_per_launch": by, "kernel_ms": kms}
