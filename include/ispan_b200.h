@@ -30,6 +30,7 @@ extern "C" {
 #define ISPAN_ERR_INTERNAL (-5)  /* a device-side capacity check failed */
 #define ISPAN_ERR_NODEV (-6)     /* no CUDA device / kernels not loadable */
 #define ISPAN_ERR_CAPACITY (-7)  /* graph larger than the context was sized for */
+#define ISPAN_ERR_BUSY (-8)      /* the server's request queue is full */
 
 /* One directed graph in the reference's CSR layout (src/graph.h:9-31):
  * fw_beg/fw_adj = out-edges, bw_beg/bw_adj = in-edges (the transpose).
@@ -62,7 +63,7 @@ typedef struct {
 #define ISPAN_F_LABELS_ON_DEVICE 1u /* labels_out is device memory */
 #define ISPAN_F_NO_GRAPH 2u         /* launch stages directly, no CUDA graph */
 #define ISPAN_F_STAGE_TIMES 4u      /* record per-stage device times */
-#define ISPAN_F_NO_L2_WINDOW 8u     /* do not pin the status maps in L2 */
+#define ISPAN_F_NO_L2_WINDOW 8u     /* no persisting L2 window over the status maps */
 #define ISPAN_F_VALIDATE 16u        /* check a device-resident CSR before the run
                                        (host CSRs are always checked) */
 #define ISPAN_F_EXACT_STATS 32u     /* also fill fw_edges / bw_edges (one extra pass) */
@@ -111,6 +112,65 @@ int ispan_scc_run(ispan_ctx *ctx, const ispan_csr *g, const ispan_params *p,
  * graph-local id).  One set of stage launches covers all graphs. */
 int ispan_scc_run_batch(ispan_ctx *ctx, const ispan_csr *g, int32_t nseg, const int64_t *vbase,
                         const ispan_params *p, int32_t *labels_out, ispan_stats *st);
+
+/* Batched form over separate graphs: gs[0..n) are independent CSRs, each on
+ * the host or the device (its own on_device) with its own offset width.  They
+ * are packed on the device into the context's union buffers (checked on the
+ * way: offsets monotone from 0 to E, ids in [0, V), else ISPAN_ERR_ARG and no
+ * stage runs), run as one disjoint union (ispan_scc_run_batch), and graph
+ * i's labels -- local min ids, as ispan_scc_run on gs[i] alone -- are written
+ * to labels_out[i] (host or device memory, told apart by address).  The sum
+ * of the graphs' V and E must fit the context; st covers the whole batch.
+ * The reference's counterpart is one scc_detection call per graph
+ * (src/scc_core.cpp:27). */
+int ispan_scc_run_graphs(ispan_ctx *ctx, const ispan_csr *gs, int32_t n, int32_t *const *labels_out,
+                         const ispan_params *p, ispan_stats *st);
+
+/* ---- served form: continuous batching over a request queue ------------
+ * No counterpart in the reference (one graph per process).  A server owns a
+ * context and a worker thread; requests are served in arrival order, each
+ * batch taking the queued requests that fit, while the caller keeps
+ * submitting.  A request's graph and label buffer must stay valid until the
+ * request is reported done. */
+typedef struct ispan_server ispan_server;
+
+typedef struct {
+    int32_t device;
+    int32_t max_batch_graphs;   /* graphs per batch; 0: 4096 */
+    int64_t hbm_budget_bytes;   /* device memory the server may hold; 0: 64 GiB */
+    int64_t max_batch_V;        /* vertices / edges per batch; 0: the largest */
+    int64_t max_batch_E;        /*   batch at 16 edges per vertex within the budget */
+    int64_t max_wait_us;        /* a partial batch waits this long for more requests */
+    int64_t max_pending;        /* queued requests before submit returns ISPAN_ERR_BUSY; 0: no limit */
+    ispan_params params;
+} ispan_server_config;
+
+typedef struct {
+    int32_t status;          /* 0 queued or running, 1 done, or an ISPAN_ERR_* code */
+    int32_t batch_graphs;    /* graphs in the batch that served it */
+    int64_t batch_id;
+    int64_t t_submit_ns;     /* CLOCK_MONOTONIC */
+    int64_t t_start_ns;      /* its batch started packing */
+    int64_t t_done_ns;       /* its labels were written */
+} ispan_request_info;
+
+/* Fails with ISPAN_ERR_NOMEM when the explicit batch size does not fit the
+ * budget. */
+int ispan_server_create(const ispan_server_config *cfg, ispan_server **out);
+int ispan_server_limits(const ispan_server *s, int64_t *max_V, int64_t *max_E, int32_t *max_graphs);
+/* Queue one graph (host or device CSR); labels_out[g->V] (host or device)
+ * receives its local min-id labels.  A graph larger than one batch is refused
+ * with ISPAN_ERR_CAPACITY. */
+int ispan_server_submit(ispan_server *s, const ispan_csr *g, int32_t *labels_out, int64_t *ticket);
+/* 1 done, 0 not yet, or the request's error; a finished request is reported
+ * once (a second poll of its ticket returns ISPAN_ERR_ARG). */
+int ispan_server_poll(ispan_server *s, int64_t ticket, ispan_request_info *info);
+/* As poll, blocking up to timeout_us (negative: no limit); 0 on timeout. */
+int ispan_server_wait(ispan_server *s, int64_t ticket, int64_t timeout_us, ispan_request_info *info);
+/* batches, graphs, vertices, edges served, busy ns, queued requests */
+int ispan_server_counters(ispan_server *s, int64_t *out, int32_t n);
+/* Serves what is queued, then stops the worker and frees the device memory. */
+int ispan_server_destroy(ispan_server *s);
 
 /* Largest graph (vertices) that ispan_scc_small_noalloc accepts. */
 #define ISPAN_NOALLOC_MAX_V 65536

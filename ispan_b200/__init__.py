@@ -24,7 +24,7 @@ from . import _lib
 from ._lib import IspanError, check
 from .graphs import CSR, read_bin
 
-__all__ = ["Context", "graph", "graph_load", "scc_detection", "get_scc_result", "print_time_result",
+__all__ = ["Context", "Server", "graph", "graph_load", "scc_detection", "get_scc_result", "print_time_result",
            "IspanError", "CSR", "scc"]
 
 REFERENCE_DEFAULTS = dict(alpha=30, beta=200, gamma=10, theta=0.1)  # src/bash_one.sh:4
@@ -152,6 +152,36 @@ class Context:
         check(rc, "ispan_scc_run")
         return labels_out, st.as_dict()
 
+    def run_graphs(self, graphs, labels_out=None, alpha=30, beta=200, gamma=10, theta=0.1,
+                   use_graph=False):
+        """Many independent graphs in one set of stage launches.  ``graphs`` is
+        a list of (fw_beg, fw_adj, bw_beg, bw_adj) -- numpy (host) or torch
+        CUDA tensors (device), each graph on its own side.  Returns one label
+        array per graph (local min ids; host graphs get numpy arrays, device
+        graphs CUDA tensors unless ``labels_out`` gives the buffers) and the
+        batch statistics."""
+        n = len(graphs)
+        arr = (_lib.Csr * n)()
+        outs = []
+        for i, (fb, fa, bb, ba) in enumerate(graphs):
+            on_dev = hasattr(fb, "is_cuda") and fb.is_cuda
+            V = (fb.numel() if hasattr(fb, "numel") else len(fb)) - 1
+            E = fa.numel() if hasattr(fa, "numel") else len(fa)
+            arr[i] = self._csr_struct(V, E, fb, fa, bb, ba, on_dev)
+            if labels_out is not None:
+                outs.append(labels_out[i])
+            elif on_dev:
+                import torch
+                outs.append(torch.empty(max(V, 1), dtype=torch.int32, device=fb.device))
+            else:
+                outs.append(np.empty(max(V, 1), np.int32))
+        ptrs = (C.c_void_p * n)(*[_ptr(o) for o in outs])
+        p = _lib.Params(alpha, beta, gamma, theta, 0 if use_graph else _lib.F_NO_GRAPH)
+        st = _lib.Stats()
+        check(_lib.lib().ispan_scc_run_graphs(self._h, arr, n, ptrs, C.byref(p), C.byref(st)),
+              "ispan_scc_run_graphs")
+        return [o[:arr[i].V] for i, o in enumerate(outs)], st.as_dict()
+
     def run_csr(self, csr: CSR, **kw):
         return self.run(csr.fw_beg, csr.fw_adj, csr.bw_beg, csr.bw_adj, V=csr.V, **kw)
 
@@ -172,6 +202,82 @@ class Context:
         out = np.empty(V + 1, np.int32)
         check(_lib.lib().ispan_ref_codes(self._h, out.ctypes.data), "ispan_ref_codes")
         return out
+
+
+class Server:
+    """Served form (ispan_server_* of include/ispan_b200.h): submit graphs one
+    at a time; a worker thread batches whatever is queued into one disjoint
+    union per batch.  Each request's arrays and label buffer must stay alive
+    until the request is reported done (the object keeps references)."""
+
+    def __init__(self, device=0, hbm_budget_bytes=0, max_batch_graphs=0, max_batch_V=0, max_batch_E=0,
+                 max_wait_us=0, max_pending=0, alpha=30, beta=200, gamma=10, theta=0.1, use_graph=False):
+        cfg = _lib.ServerConfig(device, max_batch_graphs, hbm_budget_bytes, max_batch_V, max_batch_E,
+                                max_wait_us, max_pending,
+                                _lib.Params(alpha, beta, gamma, theta, 0 if use_graph else _lib.F_NO_GRAPH))
+        h = C.c_void_p()
+        check(_lib.lib().ispan_server_create(C.byref(cfg), C.byref(h)), "ispan_server_create")
+        self._h = h
+        self._keep: dict = {}
+
+    def limits(self):
+        v, e, n = C.c_int64(), C.c_int64(), C.c_int32()
+        check(_lib.lib().ispan_server_limits(self._h, C.byref(v), C.byref(e), C.byref(n)), "limits")
+        return v.value, e.value, n.value
+
+    def submit(self, fw_beg, fw_adj, bw_beg, bw_adj, labels_out) -> int:
+        on_dev = hasattr(fw_beg, "is_cuda") and fw_beg.is_cuda
+        V = (fw_beg.numel() if hasattr(fw_beg, "numel") else len(fw_beg)) - 1
+        E = fw_adj.numel() if hasattr(fw_adj, "numel") else len(fw_adj)
+        g = Context._csr_struct(V, E, fw_beg, fw_adj, bw_beg, bw_adj, on_dev)
+        t = C.c_int64()
+        check(_lib.lib().ispan_server_submit(self._h, C.byref(g), C.c_void_p(_ptr(labels_out)), C.byref(t)),
+              "ispan_server_submit")
+        self._keep[t.value] = (fw_beg, fw_adj, bw_beg, bw_adj, labels_out)
+        return t.value
+
+    def poll(self, ticket: int):
+        """None while queued or running, else the request's info dict."""
+        info = _lib.RequestInfo()
+        rc = _lib.lib().ispan_server_poll(self._h, ticket, C.byref(info))
+        if rc == 0:
+            return None
+        self._keep.pop(ticket, None)
+        check(rc if rc < 0 else 0, "request %d" % ticket)
+        return info.as_dict()
+
+    def wait(self, ticket: int, timeout_s: float | None = None):
+        info = _lib.RequestInfo()
+        us = -1 if timeout_s is None else int(timeout_s * 1e6)
+        rc = _lib.lib().ispan_server_wait(self._h, ticket, us, C.byref(info))
+        if rc == 0:
+            return None
+        self._keep.pop(ticket, None)
+        check(rc if rc < 0 else 0, "request %d" % ticket)
+        return info.as_dict()
+
+    def counters(self) -> dict:
+        out = np.zeros(6, np.int64)
+        check(_lib.lib().ispan_server_counters(self._h, out.ctypes.data, 6), "counters")
+        return dict(zip(("batches", "graphs", "vertices", "edges", "busy_ns", "queued"), (int(x) for x in out)))
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            _lib.lib().ispan_server_destroy(self._h)
+            self._h = None
+            self._keep.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
 
 
 def scc(csr: CSR, **kw):

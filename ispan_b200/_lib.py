@@ -15,7 +15,7 @@ LIB_PATH = os.path.join(HERE, "libispan_b200_checked.so" if os.environ.get("ISPA
 
 ISPAN_OK = 0
 ERRORS = {-1: "ISPAN_ERR_ARG", -2: "ISPAN_ERR_NOMEM", -3: "ISPAN_ERR_CUDA", -4: "ISPAN_ERR_TIMEOUT",
-          -5: "ISPAN_ERR_INTERNAL", -6: "ISPAN_ERR_NODEV", -7: "ISPAN_ERR_CAPACITY"}
+          -5: "ISPAN_ERR_INTERNAL", -6: "ISPAN_ERR_NODEV", -7: "ISPAN_ERR_CAPACITY", -8: "ISPAN_ERR_BUSY"}
 
 F_LABELS_ON_DEVICE = 1
 F_NO_GRAPH = 2
@@ -58,6 +58,20 @@ class Stats(C.Structure):
         return d
 
 
+class ServerConfig(C.Structure):
+    _fields_ = [("device", C.c_int32), ("max_batch_graphs", C.c_int32), ("hbm_budget_bytes", C.c_int64),
+                ("max_batch_V", C.c_int64), ("max_batch_E", C.c_int64), ("max_wait_us", C.c_int64),
+                ("max_pending", C.c_int64), ("params", Params)]
+
+
+class RequestInfo(C.Structure):
+    _fields_ = [("status", C.c_int32), ("batch_graphs", C.c_int32), ("batch_id", C.c_int64),
+                ("t_submit_ns", C.c_int64), ("t_start_ns", C.c_int64), ("t_done_ns", C.c_int64)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 _lib = None
 
 
@@ -77,6 +91,16 @@ def lib() -> C.CDLL:
         L.ispan_scc_run.argtypes = [P, C.POINTER(Csr), C.POINTER(Params), P, C.POINTER(Stats)]
         L.ispan_scc_run_batch.argtypes = [P, C.POINTER(Csr), C.c_int32, P, C.POINTER(Params), P,
                                           C.POINTER(Stats)]
+        L.ispan_scc_run_graphs.argtypes = [P, C.POINTER(Csr), C.c_int32, P, C.POINTER(Params),
+                                           C.POINTER(Stats)]
+        L.ispan_server_create.argtypes = [C.POINTER(ServerConfig), C.POINTER(P)]
+        L.ispan_server_limits.argtypes = [P, C.POINTER(C.c_int64), C.POINTER(C.c_int64),
+                                          C.POINTER(C.c_int32)]
+        L.ispan_server_submit.argtypes = [P, C.POINTER(Csr), P, C.POINTER(C.c_int64)]
+        L.ispan_server_poll.argtypes = [P, C.c_int64, C.POINTER(RequestInfo)]
+        L.ispan_server_wait.argtypes = [P, C.c_int64, C.c_int64, C.POINTER(RequestInfo)]
+        L.ispan_server_counters.argtypes = [P, P, C.c_int32]
+        L.ispan_server_destroy.argtypes = [P]
         L.ispan_ref_codes.argtypes = [P, P]
         L.ispan_debug_trace.argtypes = [P, P, C.c_int64]
         L.ispan_scc_small_noalloc.argtypes = [C.POINTER(Csr), P, P]
@@ -88,8 +112,10 @@ def lib() -> C.CDLL:
 
 
 SYMBOLS = ("ispan_ctx_create", "ispan_ctx_destroy", "ispan_ctx_set_stream", "ispan_ctx_bytes", "ispan_scc_run",
-           "ispan_scc_run_batch", "ispan_ref_codes", "ispan_debug_trace", "ispan_scc_small_noalloc", "ispan_strerror",
-           "ispan_version")
+           "ispan_scc_run_batch", "ispan_scc_run_graphs", "ispan_server_create", "ispan_server_limits",
+           "ispan_server_submit", "ispan_server_poll", "ispan_server_wait", "ispan_server_counters",
+           "ispan_server_destroy", "ispan_ref_codes", "ispan_debug_trace", "ispan_scc_small_noalloc",
+           "ispan_strerror", "ispan_version")
 
 
 def check(rc: int, what: str = "") -> None:

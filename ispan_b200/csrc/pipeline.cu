@@ -24,6 +24,7 @@
 #include <vector>
 
 #include "bfs.cuh"
+#include "pack.cuh"
 #include "stages.cuh"
 
 using namespace ispan;
@@ -70,6 +71,20 @@ struct ispan_ctx {
     int32_t *label = nullptr;
     uint8_t *cls = nullptr;
     uint32_t *A = nullptr, *F = nullptr, *B = nullptr, *D = nullptr, *P = nullptr, *T = nullptr;
+    uint32_t *bits = nullptr;  // the block holding A..T
+    int64_t bits_bytes = 0;
+    bool l2_limit_set = false;
+
+    // union buffers of ispan_scc_run_graphs (allocated on first use)
+    int64_t *pk_fwb = nullptr, *pk_bwb = nullptr;  // [maxV + 1]
+    int32_t *pk_fwa = nullptr, *pk_bwa = nullptr;  // [maxE]
+    int64_t *pk_stage = nullptr;                   // staged host offsets [2 * (maxV + pk_n)]
+    PackDesc *pk_desc = nullptr;                   // [pk_n]
+    int64_t *pk_vb = nullptr, *pk_eb = nullptr;    // [pk_n + 1]
+    PackDesc *h_desc = nullptr;                    // pinned mirrors
+    int64_t *h_vbeb = nullptr;                     // pinned [2 * (pk_n + 1)]
+    int64_t pk_n = 0;
+    std::vector<void *> pk_owned;
     int32_t *qv[2] = {nullptr, nullptr};
     int64_t *qe[2] = {nullptr, nullptr};
     int32_t *qchunk[2] = {nullptr, nullptr};
@@ -128,7 +143,7 @@ extern "C" int64_t ispan_ctx_bytes(int64_t V, int64_t E) {
     int64_t W = words_of(V);
     int64_t b = 0;
     b += V * 4 + V;                 // label, cls
-    b += 6 * W * 4;                 // bitmaps
+    b += 6 * ((W + 63) / 64 * 64) * 4;  // bitmaps
     b += 2 * (V * 4 + (V + 1) * 8); // queues
     b += 2 * ((E / kChunk + 4) * 4);
     b += 2 * V * 4;                 // worklists
@@ -145,12 +160,18 @@ static int ctx_alloc(ispan_ctx *c) {
     auto &o = c->owned;
     rc |= dalloc(&c->label, V, o);
     rc |= dalloc(&c->cls, V, o);
-    rc |= dalloc(&c->A, W, o);
-    rc |= dalloc(&c->F, W, o);
-    rc |= dalloc(&c->B, W, o);
-    rc |= dalloc(&c->D, W, o);
-    rc |= dalloc(&c->P, W, o);
-    rc |= dalloc(&c->T, W, o);
+    // the six status maps in one block, so one L2 access-policy window covers them
+    const int64_t Wp = (W + 63) / 64 * 64;  // 256-byte aligned slices
+    rc |= dalloc(&c->bits, 6 * Wp, o);
+    c->bits_bytes = 6 * Wp * 4;
+    if (!rc) {
+        c->A = c->bits;
+        c->F = c->bits + Wp;
+        c->B = c->bits + 2 * Wp;
+        c->D = c->bits + 3 * Wp;
+        c->P = c->bits + 4 * Wp;
+        c->T = c->bits + 5 * Wp;
+    }
     for (int i = 0; i < 2; ++i) {
         rc |= dalloc(&c->qv[i], V, o);
         rc |= dalloc(&c->qe[i], V + 1, o);
@@ -339,6 +360,42 @@ static int coop_setup(ispan_ctx *c) {
     return ISPAN_OK;
 }
 
+// L2 residency of the status maps: an access-policy window over the bitmap
+// block on the run's stream (captured into the graph's kernel nodes), with
+// the device's persisting L2 carve-out raised to cover it.  The carve-out is
+// a limit of this process's context; it ends with the context.
+static void l2_window(ispan_ctx *c, bool on) {
+    int maxwin = 0, maxpersist = 0;
+    cudaDeviceGetAttribute(&maxwin, cudaDevAttrMaxAccessPolicyWindowSize, c->device);
+    cudaDeviceGetAttribute(&maxpersist, cudaDevAttrMaxPersistingL2CacheSize, c->device);
+    if (maxwin <= 0 || maxpersist <= 0 || c->bits_bytes <= 0) return;
+    const size_t bytes = std::min<size_t>((size_t)c->bits_bytes, (size_t)maxwin);
+    size_t limit = 0;
+    if (on) {
+        cudaDeviceGetLimit(&limit, cudaLimitPersistingL2CacheSize);
+        const size_t want = std::min<size_t>(bytes, (size_t)maxpersist);
+        if (limit < want) {
+            if (cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, want) != cudaSuccess) {
+                cudaGetLastError();
+                return;
+            }
+            limit = want;
+        }
+        c->l2_limit_set = true;
+    }
+    cudaStreamAttrValue v;
+    memset(&v, 0, sizeof v);
+    if (on) {
+        v.accessPolicyWindow.base_ptr = c->bits;
+        v.accessPolicyWindow.num_bytes = bytes;
+        v.accessPolicyWindow.hitRatio = std::min(1.0f, (float)limit / (float)bytes);
+        v.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
+        v.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
+    }
+    if (cudaStreamSetAttribute(c->stream, cudaStreamAttributeAccessPolicyWindow, &v) != cudaSuccess)
+        cudaGetLastError();
+}
+
 template <typename OffT>
 static int run_t(ispan_ctx *c, int64_t V, int64_t E, int32_t nseg, const OffT *fwb, const OffT *bwb,
                  const int32_t *fwa, const int32_t *bwa, int32_t *label_dev, const ispan_params *p,
@@ -379,12 +436,15 @@ static int run_t(ispan_ctx *c, int64_t V, int64_t E, int32_t nseg, const OffT *f
     // stage events are always recorded (they are nodes of the captured graph);
     // they are read back only when the caller asks for stage times
     const bool times = (flags & ISPAN_F_STAGE_TIMES) && st;
+    const bool l2win = !(flags & ISPAN_F_NO_L2_WINDOW);
+    if (l2win) l2_window(c, true);
     bool use_graph = !(flags & ISPAN_F_NO_GRAPH) && !c->graph_broken;
     if (use_graph) {
         char key[256];
         snprintf(key, sizeof key, "%d|%lld|%lld|%d|%p|%p|%p|%p|%p|%d|%d|%d|%p|%u", (int)sizeof(OffT), (long long)V,
                  (long long)E, nseg, (const void *)fwb, (const void *)bwb, (const void *)fwa, (const void *)bwa,
-                 (void *)label_dev, r.alpha, r.beta, r.gamma, (void *)c->stream, r.flags & ISPAN_F_EXACT_STATS);
+                 (void *)label_dev, r.alpha, r.beta, r.gamma, (void *)c->stream,
+                 r.flags & (ISPAN_F_EXACT_STATS | ISPAN_F_NO_L2_WINDOW));
         if (!c->gexec || strcmp(key, c->gkey) != 0) {
             if (c->gexec) {
                 cudaGraphExecDestroy(c->gexec);
@@ -418,6 +478,7 @@ static int run_t(ispan_ctx *c, int64_t V, int64_t E, int32_t nseg, const OffT *f
                        cudaMemcpyDeviceToHost, c->stream));
     CK(cudaMemcpyAsync(c->h_err, c->err, 4 * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
+    if (l2win) l2_window(c, false);  // the caller's stream gets its attribute back
 #ifdef ISPAN_CHECKED
     {
         long long chk[2] = {0, 0};
@@ -554,15 +615,13 @@ static int upload(ispan_ctx *c, const ispan_csr *g) {
     return ISPAN_OK;
 }
 
-static int run_common(ispan_ctx *c, const ispan_csr *g, int32_t nseg, const int64_t *vbase_host,
+// the body of a run; the caller holds c->mu and has made c->device current
+static int run_locked(ispan_ctx *c, const ispan_csr *g, int32_t nseg, const int64_t *vbase_host,
                       const ispan_params *p, int32_t *labels_out, ispan_stats *st) {
-    if (!c) return ISPAN_ERR_ARG;
     int rc = check_csr(g);
     if (rc) return rc;
     if (g->V > c->maxV || g->E > c->maxE) return ISPAN_ERR_CAPACITY;
     if (nseg < 1) return ISPAN_ERR_ARG;
-    std::lock_guard<std::mutex> lock(c->mu);
-    if (cudaSetDevice(c->device) != cudaSuccess) return ISPAN_ERR_CUDA;
     if ((rc = ctx_segments(c, nseg))) return rc;
     std::vector<int64_t> vb;
     if (vbase_host) {
@@ -601,6 +660,163 @@ static int run_common(ispan_ctx *c, const ispan_csr *g, int32_t nseg, const int6
         CK(cudaMemcpyAsync(labels_out, c->label, (size_t)g->V * 4, cudaMemcpyDeviceToHost, c->stream));
         CK(cudaStreamSynchronize(c->stream));
     }
+    return ISPAN_OK;
+}
+
+static int run_common(ispan_ctx *c, const ispan_csr *g, int32_t nseg, const int64_t *vbase_host,
+                      const ispan_params *p, int32_t *labels_out, ispan_stats *st) {
+    if (!c) return ISPAN_ERR_ARG;
+    std::lock_guard<std::mutex> lock(c->mu);
+    if (cudaSetDevice(c->device) != cudaSuccess) return ISPAN_ERR_CUDA;
+    return run_locked(c, g, nseg, vbase_host, p, labels_out, st);
+}
+
+// union buffers for ispan_scc_run_graphs: the CSR at the context's capacity
+// on first use, the per-graph tables grown to n
+static int pk_reserve(ispan_ctx *c, int64_t n) {
+    if (!c->pk_fwb) {
+        int rc = 0;
+        rc |= dalloc(&c->pk_fwb, c->maxV + 1, c->pk_owned);
+        rc |= dalloc(&c->pk_bwb, c->maxV + 1, c->pk_owned);
+        rc |= dalloc(&c->pk_fwa, c->maxE, c->pk_owned);
+        rc |= dalloc(&c->pk_bwa, c->maxE, c->pk_owned);
+        if (rc) {
+            for (void *q : c->pk_owned) cudaFree(q);
+            c->pk_owned.clear();
+            c->pk_fwb = c->pk_bwb = nullptr;
+            c->pk_fwa = c->pk_bwa = nullptr;
+            return ISPAN_ERR_NOMEM;
+        }
+    }
+    if (n <= c->pk_n) return ISPAN_OK;
+    const int64_t m = std::max<int64_t>({n, 2 * c->pk_n, 64});
+    // the first four allocations above stay; drop the per-graph tables
+    std::vector<void *> keep(c->pk_owned.begin(), c->pk_owned.begin() + 4);
+    for (size_t i = 4; i < c->pk_owned.size(); ++i) cudaFree(c->pk_owned[i]);
+    c->pk_owned = keep;
+    if (c->h_desc) cudaFreeHost(c->h_desc);
+    if (c->h_vbeb) cudaFreeHost(c->h_vbeb);
+    c->h_desc = nullptr;
+    c->h_vbeb = nullptr;
+    c->pk_n = 0;
+    int rc = 0;
+    rc |= dalloc(&c->pk_desc, m, c->pk_owned);
+    rc |= dalloc(&c->pk_vb, 2 * (m + 1), c->pk_owned);
+    rc |= dalloc(&c->pk_stage, 2 * (c->maxV + m), c->pk_owned);
+    if (!rc && cudaMallocHost(&c->h_desc, m * sizeof(PackDesc)) != cudaSuccess) rc = ISPAN_ERR_NOMEM;
+    if (!rc && cudaMallocHost(&c->h_vbeb, 2 * (m + 1) * sizeof(int64_t)) != cudaSuccess) rc = ISPAN_ERR_NOMEM;
+    if (rc) {
+        cudaGetLastError();
+        return ISPAN_ERR_NOMEM;
+    }
+    c->pk_eb = c->pk_vb + (m + 1);
+    c->pk_n = m;
+    return ISPAN_OK;
+}
+
+static int run_graphs(ispan_ctx *c, const ispan_csr *gs, int32_t n, int32_t *const *labels_out,
+                      const ispan_params *p, ispan_stats *st) {
+    int64_t Vt = 0, Et = 0;
+    for (int32_t i = 0; i < n; ++i) {
+        int rc = check_csr(&gs[i]);
+        if (rc) return rc;
+        if (gs[i].V > 0 && !labels_out[i]) return ISPAN_ERR_ARG;
+        Vt += gs[i].V;
+        Et += gs[i].E;
+    }
+    if (Vt > c->maxV || Et > c->maxE) return ISPAN_ERR_CAPACITY;
+    for (int32_t i = 0; i < n; ++i)
+        if (!gs[i].on_device) {
+            int rc = check_host_offsets(&gs[i]);
+            if (rc) return rc;
+        }
+    int rc = pk_reserve(c, n);
+    if (rc) return rc;
+    cudaStream_t s = c->stream;
+    // the previous batch may still read the pinned tables
+    CK(cudaStreamSynchronize(s));
+    PackDesc *hd = c->h_desc;
+    int64_t *hvb = c->h_vbeb, *heb = c->h_vbeb + (n + 1);
+    int64_t vb = 0, eb = 0, so = 0;
+    for (int32_t i = 0; i < n; ++i) {
+        const ispan_csr &g = gs[i];
+        PackDesc d;
+        memset(&d, 0, sizeof d);
+        d.V = g.V;
+        d.E = g.E;
+        d.vbase = vb;
+        d.ebase = eb;
+        d.ob = g.offset_bytes;
+        hvb[i] = vb;
+        heb[i] = eb;
+        if (g.on_device) {
+            d.fw_beg = g.fw_beg;
+            d.bw_beg = g.bw_beg;
+            d.fw_adj = g.fw_adj;
+            d.bw_adj = g.bw_adj;
+        } else {
+            // offsets staged as they are; adjacency straight into its union
+            // slice, where k_pack_adj adds the vertex base in place
+            const size_t ob = (size_t)g.offset_bytes;
+            char *st0 = reinterpret_cast<char *>(c->pk_stage + so);
+            char *st1 = reinterpret_cast<char *>(c->pk_stage + so + (g.V + 1));
+            if (g.V > 0 || g.E > 0) {
+                CK(cudaMemcpyAsync(st0, g.fw_beg, (size_t)(g.V + 1) * ob, cudaMemcpyHostToDevice, s));
+                CK(cudaMemcpyAsync(st1, g.bw_beg, (size_t)(g.V + 1) * ob, cudaMemcpyHostToDevice, s));
+            }
+            so += 2 * (g.V + 1);
+            if (g.E) {
+                CK(cudaMemcpyAsync(c->pk_fwa + eb, g.fw_adj, (size_t)g.E * 4, cudaMemcpyHostToDevice, s));
+                CK(cudaMemcpyAsync(c->pk_bwa + eb, g.bw_adj, (size_t)g.E * 4, cudaMemcpyHostToDevice, s));
+            }
+            d.fw_beg = st0;
+            d.bw_beg = st1;
+            d.fw_adj = c->pk_fwa + eb;
+            d.bw_adj = c->pk_bwa + eb;
+        }
+        hd[i] = d;
+        vb += g.V;
+        eb += g.E;
+    }
+    hvb[n] = Vt;
+    heb[n] = Et;
+    CK(cudaMemcpyAsync(c->pk_desc, hd, n * sizeof(PackDesc), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(c->pk_vb, hvb, (n + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(c->pk_eb, heb, (n + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, s));
+    CK(cudaMemsetAsync(c->err, 0, 4 * sizeof(int), s));
+    const int64_t tiles_v = Vt / kPackTile + 1, tiles_e = Et / kPackTile + 1;
+    const int gv = (int)std::min<int64_t>(tiles_v, 8 * c->nsm), ge = (int)std::min<int64_t>(tiles_e, 8 * c->nsm);
+    k_pack_offsets<<<gv, kPackThreads, 0, s>>>(c->pk_desc, n, c->pk_vb, Vt, Et, c->pk_fwb, c->pk_bwb, c->err + 1);
+    CK(cudaGetLastError());
+    if (Et > 0) {
+        k_pack_adj<<<ge, kPackThreads, 0, s>>>(c->pk_desc, n, c->pk_eb, Et, c->pk_fwa, c->pk_bwa, c->err + 1);
+        CK(cudaGetLastError());
+    }
+    CK(cudaMemcpyAsync(c->h_err, c->err, 4 * sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (c->h_err[1]) return ISPAN_ERR_ARG;
+    std::vector<int64_t> vbase(hvb, hvb + n + 1);
+    ispan_csr u;
+    memset(&u, 0, sizeof u);
+    u.V = Vt;
+    u.E = Et;
+    u.fw_beg = c->pk_fwb;
+    u.bw_beg = c->pk_bwb;
+    u.fw_adj = c->pk_fwa;
+    u.bw_adj = c->pk_bwa;
+    u.offset_bytes = 8;
+    u.on_device = 1;
+    ispan_params q = p ? *p : ispan_params{30, 200, 10, 0.1, 0};
+    q.flags = (q.flags | ISPAN_F_LABELS_ON_DEVICE) & ~(uint32_t)ISPAN_F_VALIDATE;  // packed = checked
+    if ((rc = run_locked(c, &u, n, vbase.data(), &q, c->label, st))) return rc;
+    if (Vt > 0) {
+        k_unpack_labels<<<gv, kPackThreads, 0, s>>>(c->label, n, c->pk_vb, Vt);
+        CK(cudaGetLastError());
+    }
+    for (int32_t i = 0; i < n; ++i)
+        if (gs[i].V > 0)
+            CK(cudaMemcpyAsync(labels_out[i], c->label + vbase[i], (size_t)gs[i].V * 4, cudaMemcpyDefault, s));
+    CK(cudaStreamSynchronize(s));
     return ISPAN_OK;
 }
 
@@ -653,6 +869,10 @@ int ispan_ctx_destroy(ispan_ctx *c) {
     for (void *p : c->owned) cudaFree(p);
     for (void *p : c->seg_owned) cudaFree(p);
     for (void *p : c->csr_owned) cudaFree(p);
+    for (void *p : c->pk_owned) cudaFree(p);
+    if (c->h_desc) cudaFreeHost(c->h_desc);
+    if (c->h_vbeb) cudaFreeHost(c->h_vbeb);
+    if (c->l2_limit_set) cudaCtxResetPersistingL2Cache();
     if (c->have_ev)
         for (int i = 0; i < 12; ++i) cudaEventDestroy(c->ev[i]);
     if (c->h_counters) cudaFreeHost(c->h_counters);
@@ -684,6 +904,14 @@ int ispan_scc_run_batch(ispan_ctx *c, const ispan_csr *g, int32_t nseg, const in
                         const ispan_params *p, int32_t *labels_out, ispan_stats *st) {
     if (!vbase) return ISPAN_ERR_ARG;
     return run_common(c, g, nseg, vbase, p, labels_out, st);
+}
+
+int ispan_scc_run_graphs(ispan_ctx *c, const ispan_csr *gs, int32_t n, int32_t *const *labels_out,
+                         const ispan_params *p, ispan_stats *st) {
+    if (!c || !gs || n < 1 || !labels_out) return ISPAN_ERR_ARG;
+    std::lock_guard<std::mutex> lock(c->mu);
+    if (cudaSetDevice(c->device) != cudaSuccess) return ISPAN_ERR_CUDA;
+    return run_graphs(c, gs, n, labels_out, p, st);
 }
 
 int ispan_ref_codes(ispan_ctx *c, int32_t *codes) {
@@ -733,6 +961,7 @@ const char *ispan_strerror(int code) {
         case ISPAN_ERR_INTERNAL: return "internal device-side check failed";
         case ISPAN_ERR_NODEV: return "no CUDA device";
         case ISPAN_ERR_CAPACITY: return "graph exceeds the context's capacity";
+        case ISPAN_ERR_BUSY: return "request queue full";
         default: return "unknown error";
     }
 }
