@@ -212,6 +212,51 @@ def tmpdir_for(nbytes):
     return tempfile.mkdtemp(prefix="ispan_ref_")
 
 
+def host_mem_available():
+    try:
+        with open("/proc/meminfo") as f:
+            for line in f:
+                if line.startswith("MemAvailable:"):
+                    return int(line.split()[1]) * 1024
+    except OSError:
+        pass
+    return 0
+
+
+REF_MAX_E = (1 << 31) - 1  # the reference keeps int32 offsets (src/util.h, src/graph.cpp:10-13)
+
+
+def cpu_sample_graph(workload, seed, scale, E):
+    """The graph the reference CLI can run: the workload itself, or, when its
+    edge count needs int64 offsets, the same generator at a scale that fits
+    int32 offsets (about 2^30 edges)."""
+    if E <= REF_MAX_E:
+        return None, scale
+    s = scale * (1 << 30) / E
+    g2, _ = make_graph(workload, seed, s)
+    return g2, s
+
+
+def cpu_baseline(g, args):
+    try:
+        g2, s = cpu_sample_graph(args.workload, args.seed, args.scale, g.E)
+        gg = g2 or g
+        try:
+            totals = reference_timing(gg, args.ref_steps, 1, timeout=600)
+        finally:
+            if g2 is not None:
+                g2.free()
+        cms = statistics.mean(totals)
+        sample = f"the full graph, {len(totals)} runs of the reference CLI after 1 warm-up run" if g2 is None else \
+            (f"the same generator at scale {s:.4f} ({gg.V} vertices, {gg.E} edges: the reference's int32 offsets "
+             f"cannot hold {g.E} edges), {len(totals)} runs after 1 warm-up run")
+        return {"value": gg.E / (cms / 1e3) / 1e9, "unit": "GTEPS", "cores": host_threads(), "kind": "reference",
+                "ms_per_run": cms, "sample": sample}
+    except Exception as e:  # noqa: BLE001
+        return {"value": None, "unit": "GTEPS", "cores": host_threads(), "kind": "reference",
+                "sample": f"unavailable: {str(e).splitlines()[0][:200]}"}
+
+
 def reference_timing(g, steps, warmup, timeout=900):
     """Per-run totals (ms) of the reference's unmodified CLI on this graph."""
     d = tmpdir_for(8 * g.E + 8 * g.V)
@@ -221,6 +266,68 @@ def reference_timing(g, steps, warmup, timeout=900):
     finally:
         shutil.rmtree(d, ignore_errors=True)
     return totals[warmup:] if len(totals) > warmup else totals
+
+
+def reference_per_graph(graphs_host, cap_s):
+    """The reference CLI once per graph (one warm-up + one timed run each),
+    each capped at cap_s seconds of wall time; returns (times_ms, capped)."""
+    times, capped = [], 0
+    for csr in graphs_host:
+        d = tmpdir_for(8 * csr.E + 8 * csr.V + (1 << 20))
+        try:
+            from ispan_b200.graphs import write_bin
+            paths = write_bin(csr, d, np.int32)
+            try:
+                totals, _ = run_reference_cli(paths, host_threads(), 2, cap_s)
+                times.append(totals[-1])
+            except subprocess.TimeoutExpired:
+                times.append(cap_s * 1e3)
+                capped += 1
+        finally:
+            shutil.rmtree(d, ignore_errors=True)
+    return times, capped
+
+
+def batch_sample_host(args, n, seed_shift=0):
+    """A seeded sample of the batch workload's graphs as host CSRs (int32)."""
+    from ispan_b200 import gen
+    from ispan_b200.graphs import CSR
+    nseg = max(2, int(4096 * args.scale))
+    rng = np.random.default_rng(args.seed + 99 + seed_shift)
+    pick = sorted(rng.choice(nseg, size=min(n, nseg), replace=False).tolist())
+    g = gen.batch(nseg=nseg, vmin=1000, vmax=1_000_000, ef_min=8, ef_max=32, max_cycle=1000, seed=args.seed)
+    out = []
+    for i in pick:
+        fb, fa, bb, ba = g.extract(i, "int32")
+        out.append(CSR(int(fb.numel()) - 1, int(fa.numel()), fb.cpu().numpy(), fa.cpu().numpy(),
+                       bb.cpu().numpy(), ba.cpu().numpy()))
+    g.free()
+    return pick, out
+
+
+def reference_batch_arm(args):
+    """Reference arm of the batched/served workloads: the unmodified reference
+    CLI once per graph on a seeded sample of the batch's graphs, each capped
+    (its mice stage is superlinear on planted-cycle DAGs)."""
+    try:
+        pick, graphs = batch_sample_host(args, args.ref_graphs)
+        times, capped = reference_per_graph(graphs, args.ref_cap)
+    except (FileNotFoundError, RuntimeError) as e:
+        print(json.dumps({"impl": "reference", "unavailable": str(e).splitlines()[0][:300]}))
+        return
+    gps = len(times) / (sum(times) / 1e3)
+    th = host_threads()
+    sample = (f"{len(times)} seeded graphs of the batch workload (ids {pick[:8]}...), the reference CLI once "
+              f"per graph after a warm-up run, each capped at {args.ref_cap:.0f} s ({capped} hit the cap and "
+              f"count as {args.ref_cap:.0f} s)")
+    print(json.dumps({
+        "impl": "reference", "metric": "batched graphs/s", "value": gps, "unit": "graphs/s", "n_gpus": 1,
+        "steps": len(times), "warmup": 1, "ms_per_step": sum(times) / len(times), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+        "config": {"workload": f"{args.workload} SCC, per-graph reference runs on a sample", "scale": args.scale,
+                   "parallelism": f"openmp{th}"},
+        "cpu_baseline": {"value": gps, "unit": "graphs/s", "cores": th, "kind": "reference", "sample": sample},
+        "e2e": {"value": gps, "unit": "graphs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
 
 
 # ---------------------------------------------------------------------------
@@ -288,6 +395,47 @@ def bench_batch(args, ws, rank, local):
         mism += int((out.cpu().numpy() + vb[i] != lab_host[vb[i]:vb[i + 1]]).sum())
     plain_gps = 1000.0 / statistics.mean(per_ms)
     gps = ws * nseg / (ms / 1e3)
+    # the reference CLI per graph on the first sampled graphs (capped)
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        from ispan_b200.graphs import CSR
+        hosts = []
+        for i in sample[:args.ref_graphs]:
+            a, b_, c_, d_ = g.extract(i, "int32")
+            hosts.append(CSR(int(a.numel()) - 1, int(b_.numel()), a.cpu().numpy(), b_.cpu().numpy(),
+                             c_.cpu().numpy(), d_.cpu().numpy()))
+        try:
+            times, capped = reference_per_graph(hosts, args.ref_cap)
+            cpu = {"value": len(times) / (sum(times) / 1e3), "unit": "graphs/s", "cores": host_threads(),
+                   "kind": "reference",
+                   "sample": f"{len(times)} of the sampled graphs, the reference CLI once per graph after a "
+                             f"warm-up run, capped at {args.ref_cap:.0f} s ({capped} capped)"}
+        except Exception as e:  # noqa: BLE001
+            cpu = {"value": None, "unit": "graphs/s", "cores": host_threads(), "kind": "reference",
+                   "sample": f"unavailable: {str(e).splitlines()[0][:200]}"}
+    # end to end: the union from pinned host memory through the batched call
+    e2e = None
+    h2d = 2 * (g.V + 1) * 8 + 2 * g.E * 4
+    if args.e2e_steps > 0 and host_mem_available() < 1.25 * h2d:
+        e2e = {"value": None, "unit": "graphs/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": g.V * 4,
+               "unavailable": f"host memory: {host_mem_available() / 1e9:.0f} GB available"}
+    elif args.e2e_steps > 0:
+        hfb, hfa, hbb, hba = g.to_pinned()
+        hlab = torch.empty(g.V, dtype=torch.int32, pin_memory=True)
+        np_args = [t.numpy() for t in (hfb, hfa, hbb, hba)]
+        g.free()
+        torch.cuda.empty_cache()
+        ctx.run(*np_args, V=g.V, labels_out=hlab.numpy(), vbase=vb)  # warm (upload buffers)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.e2e_steps):
+            ctx.run(*np_args, V=g.V, labels_out=hlab.numpy(), vbase=vb)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ems = max_over_ranks(e0.elapsed_time(e1), ws) / args.e2e_steps
+        e2e = {"value": ws * nseg / (ems / 1e3), "unit": "graphs/s", "ms_per_step": ems,
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": g.V * 4}
     if rank == 0:
         print(json.dumps({
             "metric": "batched graphs/s", "value": gps, "unit": "graphs/s", "n_gpus": ws, "steps": args.steps,
@@ -304,6 +452,7 @@ def bench_batch(args, ws, rank, local):
                                 "graphs_per_s": plain_gps},
             "batched_over_plain": gps / ws / plain_gps,
             "labels_batched_vs_plain_mismatches": mism,
+            "e2e": e2e, "cpu_baseline": cpu,
             "gpu_launches": KERNELS_PER_STEP * args.steps, "clocks": clk,
             "scc": {k: st[k] for k in ("scc_count", "giant_size", "n_trim1", "n_trim2", "n_trim3", "n_mice_scc",
                                        "local_wcc", "color_rounds")},
@@ -410,6 +559,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-steps", type=int, default=2, help="reference runs for cpu_baseline")
+    ap.add_argument("--ref-graphs", type=int, default=8, help="batch/served: graphs the reference runs")
+    ap.add_argument("--ref-cap", type=float, default=20.0, help="batch/served: seconds per reference graph")
     ap.add_argument("--rate", type=float, default=2000.0, help="served: requests per second")
     ap.add_argument("--duration", type=float, default=10.0, help="served: seconds of arrivals")
     ap.add_argument("--pool", type=int, default=256, help="served: distinct graphs in the request pool")
@@ -429,7 +580,15 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
+        if args.workload in ("batch", "served"):
+            return reference_batch_arm(args)
         g, desc = make_graph(args.workload, args.seed, args.scale)
+        g2, s = cpu_sample_graph(args.workload, args.seed, args.scale, g.E)
+        sample_note = ""
+        if g2 is not None:  # the reference's int32 offsets cannot hold the full graph
+            g.free()
+            g = g2
+            sample_note = f"; the same generator at scale {s:.4f} (int32 offsets of the reference)"
         try:
             totals = reference_timing(g, args.steps, args.warmup)
         except (FileNotFoundError, RuntimeError, subprocess.TimeoutExpired) as e:
@@ -438,6 +597,7 @@ def main():
         ms = statistics.mean(totals)
         val = g.E / (ms / 1e3) / 1e9
         th = host_threads()
+        desc = dict(desc, sampled_vertices=g.V, sampled_edges=g.E) if g2 is not None else desc
         print(json.dumps({
             "impl": "reference", "metric": "SCC GTEPS", "value": val, "unit": "GTEPS", "n_gpus": ws,
             "steps": len(totals), "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
@@ -445,7 +605,7 @@ def main():
             "config": dict(desc, parallelism=f"openmp{th}"),
             "cpu_baseline": {"value": val, "unit": "GTEPS", "cores": th, "kind": "reference",
                              "sample": f"full graph, {len(totals)} timed runs of the reference CLI "
-                                       f"(src/scc_main.cpp) after {args.warmup} warm-up runs"},
+                                       f"(src/scc_main.cpp) after {args.warmup} warm-up runs{sample_note}"},
             "e2e": {"value": val, "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
         return
 
@@ -455,9 +615,9 @@ def main():
     stream = torch.cuda.Stream()
     ctx = Context(g.V, g.E)
     ctx.set_stream(stream)
-    fb, fa, bb, ba = g.to_torch("int64")
+    fb, fa, bb, ba = g.ptrs  # the generator's device arrays, no copy
     labels = torch.empty(g.V, dtype=torch.int32, device="cuda")
-    run = lambda: ctx.run(fb, fa, bb, ba, V=g.V, labels_out=labels, stage_times=True)  # noqa: E731
+    run = lambda: ctx.run_raw(g.V, g.E, fb, fa, bb, ba, 8, labels, stage_times=True)  # noqa: E731
     for _ in range(args.warmup):
         _, st = run()
     torch.cuda.synchronize()
@@ -485,7 +645,7 @@ def main():
 
     # roofline of the dominant kernel (the longer of the FW and BW searches);
     # the degree sums of the reached sets come from one extra, untimed run
-    _, st_x = ctx.run(fb, fa, bb, ba, V=g.V, labels_out=labels, exact_stats=True)
+    _, st_x = ctx.run_raw(g.V, g.E, fb, fa, bb, ba, 8, labels, exact_stats=True)
     st = dict(st, fw_edges=st_x["fw_edges"], bw_edges=st_x["bw_edges"])
     fw_b, bw_b = alg_bytes(st)
     fw_ms = statistics.mean(s["stage_ms"][7] for s in stages)
@@ -502,20 +662,23 @@ def main():
             "alg_bytes_per_launch": by, "kernel_ms": kms}
     stage_mean = [statistics.mean(s["stage_ms"][i] for s in stages) for i in range(16)]
 
+    # ---- CPU baseline: the reference's own OpenMP build on this host ----
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(g, args)
+
     # ---- end to end through the public API with pinned host buffers ----
     e2e = None
-    if args.e2e_steps > 0:
-        hfb = torch.empty(g.V + 1, dtype=torch.int64, pin_memory=True)
-        hbb = torch.empty(g.V + 1, dtype=torch.int64, pin_memory=True)
-        hfa = torch.empty(g.E, dtype=torch.int32, pin_memory=True)
-        hba = torch.empty(g.E, dtype=torch.int32, pin_memory=True)
-        hfb.copy_(fb)
-        hbb.copy_(bb)
-        hfa.copy_(fa)
-        hba.copy_(ba)
+    h2d = 2 * (g.V + 1) * 8 + 2 * g.E * 4
+    if args.e2e_steps > 0 and host_mem_available() < 1.25 * h2d:
+        e2e = {"value": None, "unit": "GTEPS", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": g.V * 4,
+               "unavailable": f"host memory: {host_mem_available() / 1e9:.0f} GB available, "
+                              f"{h2d / 1e9:.0f} GB of pinned input needed"}
+    elif args.e2e_steps > 0:
+        hfb, hfa, hbb, hba = g.to_pinned()
         hlab = torch.empty(g.V, dtype=torch.int32, pin_memory=True)
         np_args = [t.numpy() for t in (hfb, hfa, hbb, hba)]
-        del fb, fa, bb, ba
+        g.free()  # the upload buffers take the generator's place on the device
         torch.cuda.empty_cache()
         ctx.run(*np_args, V=g.V, labels_out=hlab.numpy())  # warm (allocates the upload buffers)
         barrier(ws)
@@ -527,22 +690,8 @@ def main():
         e1.record(stream)
         torch.cuda.synchronize()
         e2e_ms = max_over_ranks(e0.elapsed_time(e1), ws) / args.e2e_steps
-        h2d = 2 * (g.V + 1) * 8 + 2 * g.E * 4
         e2e = {"value": ws * g.E / (e2e_ms / 1e3) / 1e9, "unit": "GTEPS", "ms_per_step": e2e_ms,
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": g.V * 4}
-
-    # ---- CPU baseline: the reference's own OpenMP build on this host ----
-    cpu = None
-    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
-        try:
-            totals = reference_timing(g, args.ref_steps, 1, timeout=600)
-            cms = statistics.mean(totals)
-            cpu = {"value": g.E / (cms / 1e3) / 1e9, "unit": "GTEPS", "cores": host_threads(),
-                   "kind": "reference", "ms_per_run": cms,
-                   "sample": f"the full graph, {len(totals)} runs of the reference CLI after 1 warm-up run"}
-        except Exception as e:  # noqa: BLE001
-            cpu = {"value": None, "unit": "GTEPS", "cores": host_threads(), "kind": "reference",
-                   "sample": f"unavailable: {str(e).splitlines()[0][:200]}"}
 
     if rank == 0:
         out = {

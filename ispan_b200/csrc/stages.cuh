@@ -898,6 +898,7 @@ constexpr int kCLQ = 2048;
 struct ColorSmem {
     int32_t lq[2][kCLQ];
     int cnt[2];
+    int take;  // slice entries joining the next level
 };
 
 // One asynchronous round over the global queue q_in[0..n_in).  KIND 0
@@ -914,17 +915,25 @@ __device__ __forceinline__ void color_async_round(const Run<OffT> &r, const Ext<
     const OffT *beg = KIND == 0 ? r.fw_beg : r.bw_beg;
     const int32_t *adj = KIND == 0 ? r.fw_adj : r.bw_adj;
     const int tid = threadIdx.x;
+    // This CTA's slice of the queue feeds its local frontier as room frees
+    // up, so the searches started from all of the slice's entries advance
+    // together, level by level (working the slice in separate chunks would
+    // pay the depth of a search once per chunk).
     const int64_t s0 = n_in * blockIdx.x / gridDim.x, s1 = n_in * (blockIdx.x + 1) / gridDim.x;
-    for (int64_t bs = s0; bs < s1; bs += kCLQ) {
-        const int n0 = (int)min((int64_t)kCLQ, s1 - bs);
+    int64_t next_in = s0;
+    {
+        const int n0 = (int)min((int64_t)kCLQ, s1 - s0);
         __syncthreads();
-        for (int i = tid; i < n0; i += kBlock) sm.lq[0][i] = __ldcg(q_in + bs + i);
+        for (int i = tid; i < n0; i += kBlock) sm.lq[0][i] = __ldcg(q_in + s0 + i);
         if (tid == 0) { sm.cnt[0] = n0; sm.cnt[1] = 0; }
+        next_in += n0;
         __syncthreads();
+    }
+    {
         int c = 0;
-        for (int it = 0; it < (1 << 20); ++it) {
+        for (int it = 0; it < (1 << 30); ++it) {
             const int n = sm.cnt[c];
-            if (n == 0) break;
+            if (n == 0) break;  // the slice is consumed too (the refill keeps the frontier non-empty)
             for (int i = tid; i < n; i += kBlock) {
                 const int32_t v = sm.lq[c][i];
                 uint32_t cv;
@@ -971,8 +980,17 @@ __device__ __forceinline__ void color_async_round(const Run<OffT> &r, const Ext<
             }
             __syncthreads();
             if (tid == 0) {
-                sm.cnt[c ^ 1] = min(sm.cnt[c ^ 1], kCLQ);
+                const int m = min(sm.cnt[c ^ 1], kCLQ);
+                const int take = (int)min((int64_t)(kCLQ - m), s1 - next_in);
+                sm.cnt[c ^ 1] = m + take;
+                sm.take = take;
                 sm.cnt[c] = 0;
+            }
+            __syncthreads();
+            {
+                const int take = sm.take, m = sm.cnt[c ^ 1] - take;
+                for (int i = tid; i < take; i += kBlock) sm.lq[c ^ 1][m + i] = __ldcg(q_in + next_in + i);
+                next_in += take;
             }
             __syncthreads();
             c ^= 1;

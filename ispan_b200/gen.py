@@ -64,6 +64,18 @@ class DeviceGraph:
             raise RuntimeError(f"ispan_gen_copy failed ({rc})")
         return CSR(self.V, self.E, fb, fa[:self.E], bb, ba[:self.E])
 
+    def to_pinned(self):
+        """Copies in pinned host memory as CPU tensors (int64 offsets)."""
+        import torch
+        fb = torch.empty(self.V + 1, dtype=torch.int64, pin_memory=True)
+        bb = torch.empty(self.V + 1, dtype=torch.int64, pin_memory=True)
+        fa = torch.empty(max(self.E, 1), dtype=torch.int32, pin_memory=True)
+        ba = torch.empty(max(self.E, 1), dtype=torch.int32, pin_memory=True)
+        rc = lib().ispan_gen_copy(self._h, fb.data_ptr(), fa.data_ptr(), bb.data_ptr(), ba.data_ptr(), 8, 0)
+        if rc:
+            raise RuntimeError(f"ispan_gen_copy failed ({rc})")
+        return fb, fa[:self.E], bb, ba[:self.E]
+
     def to_torch(self, offset_dtype="int64"):
         """Copies as CUDA tensors (fw_beg, fw_adj, bw_beg, bw_adj)."""
         import torch
