@@ -99,6 +99,22 @@ int ispan_ctx_set_stream(ispan_ctx *ctx, void *cuda_stream);
 /* device bytes a context of this size holds (without uploaded graphs) */
 int64_t ispan_ctx_bytes(int64_t max_V, int64_t max_E);
 
+/* Launch tunables of a context, chosen per graph-shape class by the
+ * autotuner (ispan_b200/autotune.py).  They change scheduling only, never
+ * labels.  Zero fields take the defaults.  The reference's only knobs are
+ * alpha/beta/gamma/theta (src/scc_main.cpp:16-25); these have no counterpart. */
+typedef struct {
+    int64_t async_v;          /* a search goes asynchronous below this many frontier vertices (65536) */
+    int64_t async_e;          /* ... and this many frontier edges (262144) */
+    int32_t async_deg;        /* an asynchronous CTA expands vertices up to this degree itself (16) */
+    int32_t bfs_ctas_per_sm;  /* CTAs per SM of the persistent searches, at most the occupancy limit (2) */
+} ispan_tuning;
+
+/* NULL restores the defaults; the next run re-captures its CUDA graph. */
+int ispan_ctx_set_tuning(ispan_ctx *ctx, const ispan_tuning *t);
+/* the values in effect (defaults filled in; bfs_ctas_per_sm 0 = occupancy limit) */
+int ispan_ctx_get_tuning(ispan_ctx *ctx, ispan_tuning *t);
+
 /* Detect the SCCs of g.  labels_out[V] receives, for every vertex, the
  * minimum vertex id of its SCC (host memory unless ISPAN_F_LABELS_ON_DEVICE).
  * Replaces scc_detection (src/scc_core.cpp:27); st may be NULL. */

@@ -58,6 +58,14 @@ class Stats(C.Structure):
         return d
 
 
+class Tuning(C.Structure):
+    _fields_ = [("async_v", C.c_int64), ("async_e", C.c_int64), ("async_deg", C.c_int32),
+                ("bfs_ctas_per_sm", C.c_int32)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class ServerConfig(C.Structure):
     _fields_ = [("device", C.c_int32), ("max_batch_graphs", C.c_int32), ("hbm_budget_bytes", C.c_int64),
                 ("max_batch_V", C.c_int64), ("max_batch_E", C.c_int64), ("max_wait_us", C.c_int64),
@@ -91,6 +99,8 @@ def lib() -> C.CDLL:
         L.ispan_scc_run.argtypes = [P, C.POINTER(Csr), C.POINTER(Params), P, C.POINTER(Stats)]
         L.ispan_scc_run_batch.argtypes = [P, C.POINTER(Csr), C.c_int32, P, C.POINTER(Params), P,
                                           C.POINTER(Stats)]
+        L.ispan_ctx_set_tuning.argtypes = [P, C.POINTER(Tuning)]
+        L.ispan_ctx_get_tuning.argtypes = [P, C.POINTER(Tuning)]
         L.ispan_scc_run_graphs.argtypes = [P, C.POINTER(Csr), C.c_int32, P, C.POINTER(Params),
                                            C.POINTER(Stats)]
         L.ispan_server_create.argtypes = [C.POINTER(ServerConfig), C.POINTER(P)]
@@ -112,7 +122,7 @@ def lib() -> C.CDLL:
 
 
 SYMBOLS = ("ispan_ctx_create", "ispan_ctx_destroy", "ispan_ctx_set_stream", "ispan_ctx_bytes", "ispan_scc_run",
-           "ispan_scc_run_batch", "ispan_scc_run_graphs", "ispan_server_create", "ispan_server_limits",
+           "ispan_scc_run_batch", "ispan_scc_run_graphs", "ispan_ctx_set_tuning", "ispan_ctx_get_tuning", "ispan_server_create", "ispan_server_limits",
            "ispan_server_submit", "ispan_server_poll", "ispan_server_wait", "ispan_server_counters",
            "ispan_server_destroy", "ispan_ref_codes", "ispan_debug_trace", "ispan_scc_small_noalloc",
            "ispan_strerror", "ispan_version")

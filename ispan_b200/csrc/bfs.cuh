@@ -33,10 +33,10 @@ namespace ispan {
 
 constexpr int kBuLane = 16;          // edges a lane scans alone in bottom-up
 constexpr int kLQ = 2048;               // per-CTA local frontier (shared memory) in the async mode
-constexpr int kAsyncDeg = 16;           // vertices up to this degree are expanded locally
+constexpr int kAsyncDeg = 16;           // default of Run::async_deg: vertices up to this degree are expanded locally
 constexpr int kAsyncMaxLevels = 4096;   // local levels before a CTA hands its frontier back
-constexpr int64_t kAsyncV = 65536;      // frontier size that enters the async mode ...
-constexpr int64_t kAsyncE = 262144;     // ... and frontier edges
+constexpr int64_t kAsyncV = 65536;      // defaults of Run::async_v: frontier size that enters the async mode ...
+constexpr int64_t kAsyncE = 262144;     // ... and Run::async_e: frontier edges
 
 enum BfsMode : int { M_TD = 0, M_BU = 1, M_ASYNC = 2, M_DONE = 3 };
 
@@ -387,7 +387,7 @@ __device__ __forceinline__ void async_round(const Run<OffT> &r, const BfsDir<Off
                         nvis += 1;
                         msum_other += d.odeg(w[q]);
                         if (dg == 0) continue;
-                        int pos = dg <= kAsyncDeg ? atomicAdd(&sm.cnt[c ^ 1], 1) : kLQ;
+                        int pos = dg <= r.async_deg ? atomicAdd(&sm.cnt[c ^ 1], 1) : kLQ;
                         if (pos < kLQ) {
                             sm.lq[c ^ 1][pos] = w[q];
                         } else {  // a hub, or the local frontier is full
@@ -451,7 +451,8 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Run<OffT> r, BfsCtl *ctl) {
     bool left_bu = false;  // like the reference, a search never returns to bottom-up
     int64_t total_vis = 0;
     // small frontiers go to the async mode; larger ones stay top-down
-    auto small = [](int64_t qc, int64_t qe) { return qc <= kAsyncV && qe <= kAsyncE; };
+    const int64_t av = r.async_v, ae = r.async_e;
+    auto small = [av, ae](int64_t qc, int64_t qe) { return qc <= av && qe <= ae; };
 
     for (int guard = 0; guard < (1 << 30); ++guard) {
         const int cur = level & 1;

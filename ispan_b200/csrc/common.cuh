@@ -66,6 +66,8 @@ struct Run {
     int *err;                     // [4] error word, detail
     int32_t alpha, beta, gamma;
     uint32_t flags;
+    int64_t async_v, async_e;     // a search goes asynchronous below these frontier sizes
+    int32_t async_deg;            // degree up to which an asynchronous CTA expands a vertex itself
 };
 
 // statistics counters (indices into Run::counters)

@@ -110,6 +110,8 @@ struct ispan_ctx {
     unsigned long long *h_counters = nullptr;  // pinned
     int *h_err = nullptr;
 
+    ispan_tuning tuning = {0, 0, 0, 0};
+
     // launch geometry
     int g_stream = 0;           // grid for plain grid-stride kernels
     int g_coop[4] = {0, 0, 0, 0};  // bfs<0>, bfs<1>, trim1, color (per offset width)
@@ -272,6 +274,9 @@ static void fill_run(ispan_ctx *c, Run<OffT> &r, Ext<OffT> &x, int64_t V, int64_
     r.beta = p && p->beta > 0 ? p->beta : 200;
     r.gamma = p && p->gamma > 0 ? p->gamma : 10;
     r.flags = p ? p->flags : 0;
+    r.async_v = c->tuning.async_v > 0 ? c->tuning.async_v : kAsyncV;
+    r.async_e = c->tuning.async_e > 0 ? c->tuning.async_e : kAsyncE;
+    r.async_deg = c->tuning.async_deg > 0 ? c->tuning.async_deg : kAsyncDeg;
     x.ctl = c->ctlblk + kCtlX;
     x.roots = c->roots;
     x.small = c->small;
@@ -352,6 +357,10 @@ static int coop_setup(ispan_ctx *c) {
     if (c->g_coop_w == w) return ISPAN_OK;
     c->g_coop[0] = coop_grid(k_bfs<OffT, 0>, c->nsm, kBlock);
     c->g_coop[1] = coop_grid(k_bfs<OffT, 1>, c->nsm, kBlock);
+    // fewer CTAs per SM than the occupancy limit on request (never more)
+    const int want = c->tuning.bfs_ctas_per_sm;
+    if (want > 0)
+        for (int i = 0; i < 2; ++i) c->g_coop[i] = std::min(c->g_coop[i], want * c->nsm);
     c->g_coop[2] = coop_grid(k_trim1<OffT>, c->nsm, kBlock);
     c->g_coop[3] = coop_grid(k_color<OffT>, c->nsm, kBlock);
     for (int i = 0; i < 4; ++i)
@@ -892,6 +901,30 @@ int ispan_ctx_set_stream(ispan_ctx *c, void *stream) {
         cudaGraphExecDestroy(c->gexec);
         c->gexec = nullptr;
     }
+    return ISPAN_OK;
+}
+
+int ispan_ctx_set_tuning(ispan_ctx *c, const ispan_tuning *t) {
+    if (!c) return ISPAN_ERR_ARG;
+    if (t && (t->async_v < 0 || t->async_e < 0 || t->async_deg < 0 || t->bfs_ctas_per_sm < 0))
+        return ISPAN_ERR_ARG;
+    std::lock_guard<std::mutex> lock(c->mu);
+    c->tuning = t ? *t : ispan_tuning{0, 0, 0, 0};
+    c->g_coop_w = 0;  // recompute the persistent grids
+    if (c->gexec) {   // the captured graph holds the old values
+        cudaGraphExecDestroy(c->gexec);
+        c->gexec = nullptr;
+    }
+    return ISPAN_OK;
+}
+
+int ispan_ctx_get_tuning(ispan_ctx *c, ispan_tuning *t) {
+    if (!c || !t) return ISPAN_ERR_ARG;
+    std::lock_guard<std::mutex> lock(c->mu);
+    t->async_v = c->tuning.async_v > 0 ? c->tuning.async_v : kAsyncV;
+    t->async_e = c->tuning.async_e > 0 ? c->tuning.async_e : kAsyncE;
+    t->async_deg = c->tuning.async_deg > 0 ? c->tuning.async_deg : kAsyncDeg;
+    t->bfs_ctas_per_sm = c->tuning.bfs_ctas_per_sm;
     return ISPAN_OK;
 }
 

@@ -114,3 +114,19 @@ def test_reference_codes_report(ctx):
     codes = ctx.ref_codes(csr.V)
     assert codes[csr.V] == 0
     assert np.array_equal(oracle.canon_codes(csr, codes), oracle.tarjan(csr))
+
+
+@pytest.mark.parametrize("tun", [dict(async_v=1, async_e=1, async_deg=1, bfs_ctas_per_sm=1),
+                                 dict(async_v=1 << 22, async_e=1 << 24, async_deg=1024),
+                                 dict(async_v=4096, async_e=16384, async_deg=4)])
+def test_tuning_does_not_change_labels(tun):
+    """The autotuner's launch parameters move time between stages only."""
+    with Context(1 << 17, 1 << 21) as c:
+        c.set_tuning(**tun)
+        for g in (G.rmat(14, 16, 9), G.planted(20000, 8, giant_frac=0.3), G.planted(30000, 9, giant_frac=0.0,
+                                                                                      dag_ef=3.0, max_cycle=300)):
+            for a, b, gm in ((30, 200, 10), (3, 4000, 3), (300, 50, 30)):
+                labels, _ = c.run_csr(g, alpha=a, beta=b, gamma=gm)
+                assert np.array_equal(labels, oracle.tarjan(g))
+        t = c.tuning()
+        assert t["async_deg"] == tun["async_deg"]
