@@ -142,20 +142,34 @@ int ispan_scc_run_batch(ispan_ctx *ctx, const ispan_csr *g, int32_t nseg, const 
 int ispan_scc_run_graphs(ispan_ctx *ctx, const ispan_csr *gs, int32_t n, int32_t *const *labels_out,
                          const ispan_params *p, ispan_stats *st);
 
+/* The two phases of ispan_scc_run_graphs, for callers that overlap them:
+ * pack copies and checks the graphs into the context's union buffers (host
+ * copies, then two short kernels on the context's stream); run executes the
+ * pipeline on the packed union and writes the labels.  A server packs batch
+ * k+1 on one context while batch k runs on another.  run must get the same
+ * gs sizes as the pack before it, else ISPAN_ERR_ARG. */
+int ispan_graphs_pack(ispan_ctx *ctx, const ispan_csr *gs, int32_t n);
+int ispan_graphs_run(ispan_ctx *ctx, const ispan_csr *gs, int32_t n, int32_t *const *labels_out,
+                     const ispan_params *p, ispan_stats *st);
+
 /* ---- served form: continuous batching over a request queue ------------
- * No counterpart in the reference (one graph per process).  A server owns a
- * context and a worker thread; requests are served in arrival order, each
- * batch taking the queued requests that fit, while the caller keeps
- * submitting.  A request's graph and label buffer must stay valid until the
- * request is reported done. */
+ * No counterpart in the reference (one graph per process).  A server owns
+ * n_slots batch slots (a context each, the budget split between them) and a
+ * worker thread per slot.  Requests are served in arrival order; a slot takes
+ * the queued requests that fit when the device is idle or a full batch is
+ * waiting, packs them while another slot's batch runs, and runs when the
+ * device frees (one pipeline on the device at a time).  A request's graph and
+ * label buffer must stay valid until the request is reported done. */
 typedef struct ispan_server ispan_server;
 
 typedef struct {
     int32_t device;
     int32_t max_batch_graphs;   /* graphs per batch; 0: 4096 */
+    int32_t n_slots;            /* batch slots (contexts) sharing the budget; 0: 2 */
+    int32_t reserved;
     int64_t hbm_budget_bytes;   /* device memory the server may hold; 0: 64 GiB */
-    int64_t max_batch_V;        /* vertices / edges per batch; 0: the largest */
-    int64_t max_batch_E;        /*   batch at 16 edges per vertex within the budget */
+    int64_t max_batch_V;        /* vertices / edges per batch (one slot); 0: the */
+    int64_t max_batch_E;        /*   largest at 16 edges per vertex within the slot's share */
     int64_t max_wait_us;        /* a partial batch waits this long for more requests */
     int64_t max_pending;        /* queued requests before submit returns ISPAN_ERR_BUSY; 0: no limit */
     ispan_params params;

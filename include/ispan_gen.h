@@ -70,6 +70,16 @@ int ispan_gen_device_ptrs(const ispan_gen_graph *g, const int64_t **fw_beg, cons
 int ispan_gen_extract(const ispan_gen_graph *g, int64_t vlo, int64_t vhi, void *fw_beg, int32_t *fw_adj,
                       void *bw_beg, int32_t *bw_adj, int32_t offset_bytes, int64_t *E_out);
 
+/* The SCC partition the social and web generators plant, as canonical
+ * labels (minimum vertex id of each planted SCC) into labels[V] (device
+ * memory).  By construction it is the graph's exact SCC partition: the
+ * core is strongly connected through its Hamiltonian cycle, every small
+ * cycle / planted SCC is attached to the rest in one direction only, and
+ * sources, sinks and DAG vertices have no path back.  This gives an exact
+ * check at full size, where a CPU Tarjan would take minutes.  -4 for
+ * generators without a planted partition (R-MAT, batch). */
+int ispan_gen_planted_labels(const ispan_gen_graph *g, int32_t *labels);
+
 int ispan_gen_free(ispan_gen_graph *g);
 
 #ifdef __cplusplus

@@ -221,8 +221,9 @@ class Server:
     until the request is reported done (the object keeps references)."""
 
     def __init__(self, device=0, hbm_budget_bytes=0, max_batch_graphs=0, max_batch_V=0, max_batch_E=0,
-                 max_wait_us=0, max_pending=0, alpha=30, beta=200, gamma=10, theta=0.1, use_graph=False):
-        cfg = _lib.ServerConfig(device, max_batch_graphs, hbm_budget_bytes, max_batch_V, max_batch_E,
+                 max_wait_us=0, max_pending=0, alpha=30, beta=200, gamma=10, theta=0.1, use_graph=False,
+                 n_slots=0):
+        cfg = _lib.ServerConfig(device, max_batch_graphs, n_slots, 0, hbm_budget_bytes, max_batch_V, max_batch_E,
                                 max_wait_us, max_pending,
                                 _lib.Params(alpha, beta, gamma, theta, 0 if use_graph else _lib.F_NO_GRAPH))
         h = C.c_void_p()

@@ -67,7 +67,8 @@ class Tuning(C.Structure):
 
 
 class ServerConfig(C.Structure):
-    _fields_ = [("device", C.c_int32), ("max_batch_graphs", C.c_int32), ("hbm_budget_bytes", C.c_int64),
+    _fields_ = [("device", C.c_int32), ("max_batch_graphs", C.c_int32), ("n_slots", C.c_int32),
+                ("reserved", C.c_int32), ("hbm_budget_bytes", C.c_int64),
                 ("max_batch_V", C.c_int64), ("max_batch_E", C.c_int64), ("max_wait_us", C.c_int64),
                 ("max_pending", C.c_int64), ("params", Params)]
 
@@ -103,6 +104,8 @@ def lib() -> C.CDLL:
         L.ispan_ctx_get_tuning.argtypes = [P, C.POINTER(Tuning)]
         L.ispan_scc_run_graphs.argtypes = [P, C.POINTER(Csr), C.c_int32, P, C.POINTER(Params),
                                            C.POINTER(Stats)]
+        L.ispan_graphs_pack.argtypes = [P, C.POINTER(Csr), C.c_int32]
+        L.ispan_graphs_run.argtypes = [P, C.POINTER(Csr), C.c_int32, P, C.POINTER(Params), C.POINTER(Stats)]
         L.ispan_server_create.argtypes = [C.POINTER(ServerConfig), C.POINTER(P)]
         L.ispan_server_limits.argtypes = [P, C.POINTER(C.c_int64), C.POINTER(C.c_int64),
                                           C.POINTER(C.c_int32)]
@@ -122,7 +125,7 @@ def lib() -> C.CDLL:
 
 
 SYMBOLS = ("ispan_ctx_create", "ispan_ctx_destroy", "ispan_ctx_set_stream", "ispan_ctx_bytes", "ispan_scc_run",
-           "ispan_scc_run_batch", "ispan_scc_run_graphs", "ispan_ctx_set_tuning", "ispan_ctx_get_tuning", "ispan_server_create", "ispan_server_limits",
+           "ispan_scc_run_batch", "ispan_scc_run_graphs", "ispan_graphs_pack", "ispan_graphs_run", "ispan_ctx_set_tuning", "ispan_ctx_get_tuning", "ispan_server_create", "ispan_server_limits",
            "ispan_server_submit", "ispan_server_poll", "ispan_server_wait", "ispan_server_counters",
            "ispan_server_destroy", "ispan_ref_codes", "ispan_debug_trace", "ispan_scc_small_noalloc",
            "ispan_strerror", "ispan_version")

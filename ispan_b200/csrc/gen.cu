@@ -24,11 +24,13 @@
 
 #include "../../include/ispan_gen.h"
 
+struct PlantedInfo;
 struct ispan_gen_graph {
     int device = 0;
     int64_t V = 0, E = 0;
     int64_t *fw_beg = nullptr, *bw_beg = nullptr;
     int32_t *fw_adj = nullptr, *bw_adj = nullptr;
+    PlantedInfo *planted = nullptr;  // the SCC partition the generator planted (social, web)
 };
 
 namespace {
@@ -150,6 +152,51 @@ struct PowerLaw {
         return make(n, beta, sqrt(lo * hi));
     }
 };
+
+// ---------------------------------------------------------------------------
+// The SCC partition a generator planted, in rank space: the core [0, n_core)
+// is one SCC, the ranks [block_lo, block_lo + bnd.back()) are cut into SCCs
+// at the relative boundaries bnd, every other rank is an SCC of its own.  A
+// vertex's planted label is the minimum vertex id of its SCC.
+}  // namespace
+
+struct PlantedInfo {  // declared with ispan_gen_graph, outside the file's unnamed namespace
+    Perm perm;
+    int64_t n = 0, n_core = 0, block_lo = 0;
+    std::vector<int64_t> bnd;
+};
+
+namespace {
+
+__device__ __forceinline__ int64_t planted_group(int64_t r, int64_t n_core, int64_t block_lo, const int64_t *bnd,
+                                                 int64_t nb) {
+    if (r < n_core) return 0;
+    const int64_t x = r - block_lo;
+    if (x < 0 || x >= bnd[nb]) return -1;
+    int64_t lo = 0, hi = nb - 1;
+    while (lo < hi) {
+        int64_t mid = (lo + hi + 1) >> 1;
+        if (bnd[mid] <= x) lo = mid; else hi = mid - 1;
+    }
+    return 1 + lo;
+}
+
+__global__ void k_planted_min(Perm perm, int64_t n, int64_t n_core, int64_t block_lo, const int64_t *bnd,
+                              int64_t nb, int32_t *gmin) {
+    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t gi = planted_group(r, n_core, block_lo, bnd, nb);
+        if (gi >= 0) atomicMin(gmin + gi, (int32_t)perm.vertex(r));
+    }
+}
+
+__global__ void k_planted_label(Perm perm, int64_t n, int64_t n_core, int64_t block_lo, const int64_t *bnd,
+                                int64_t nb, const int32_t *gmin, int32_t *label) {
+    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t gi = planted_group(r, n_core, block_lo, bnd, nb);
+        const int64_t v = perm.vertex(r);
+        label[v] = gi >= 0 ? gmin[gi] : (int32_t)v;
+    }
+}
 
 // ---------------------------------------------------------------------------
 // social-network edge program
@@ -443,6 +490,7 @@ struct WebProg {
     int64_t n_core, n_src, n_snk, n_scc_v, n_scc;
     int64_t b_src, b_snk, b_scc;
     int64_t core_extra, src_e, snk_e, dag_e;
+    int64_t half;  // SCC-block rank where edges to the core stop and edges from it start (an SCC boundary)
     int64_t cat_begin[W_NCAT + 1];
     const int64_t *scc_off;   // [n_scc+1] rank offsets inside the SCC block
     const int64_t *scc_item;  // [n_scc+1] item prefix (ring + chords)
@@ -496,7 +544,7 @@ __global__ void k_web(WebProg P, uint64_t *keys, int64_t total) {
                 int64_t y = (int64_t)(rnd(s, cat, j, 1) % (uint64_t)P.n_scc_v);
                 uint64_t h = rnd(s, cat, j, 2);
                 if ((h & 7) == 0) {
-                    if (x < P.n_scc_v / 2)
+                    if (x < P.half)
                         key = key_of(P.perm, P.b_scc + x, (int64_t)(rnd(s, cat, j, 3) % (uint64_t)P.n_core));
                     else
                         key = key_of(P.perm, (int64_t)(rnd(s, cat, j, 3) % (uint64_t)P.n_core), P.b_scc + x);
@@ -675,6 +723,18 @@ int ispan_gen_social(int device, int64_t n, int64_t edges, double giant_frac, do
     cudaFree(d_toff);
     cudaFree(d_titem);
     if (rc) { ispan_gen_free(g); return rc; }
+    {   // core; then pairs, triangles and tail cycles are contiguous from b_pair
+        PlantedInfo *pi = new PlantedInfo();
+        pi->perm = P.perm;
+        pi->n = n;
+        pi->n_core = P.n_core;
+        pi->block_lo = P.b_pair;
+        pi->bnd.push_back(0);
+        for (int64_t k = 0; k < n_pair; ++k) pi->bnd.push_back(pi->bnd.back() + 2);
+        for (int64_t k = 0; k < n_tri; ++k) pi->bnd.push_back(pi->bnd.back() + 3);
+        for (int64_t k = 0; k < n_tail; ++k) pi->bnd.push_back(pi->bnd.back() + (toff[k + 1] - toff[k]));
+        g->planted = pi;
+    }
     *out = g;
     return 0;
 }
@@ -701,6 +761,9 @@ int ispan_gen_web(int device, int64_t n, int64_t edges, double giant_frac, doubl
     }
     P.n_scc = (int64_t)off.size() - 1;
     P.n_scc_v = rest;
+    // no planted SCC may have members on both sides of the split, or it
+    // would reach the core and be reached from it (and join the giant)
+    P.half = *std::lower_bound(off.begin(), off.end(), rest / 2);
     P.n_src = n_triv / 2;
     P.n_snk = n_triv - P.n_src;
     P.b_src = P.n_core;
@@ -735,6 +798,15 @@ int ispan_gen_web(int device, int64_t n, int64_t edges, double giant_frac, doubl
     cudaFree(d_off);
     cudaFree(d_item);
     if (rc) { ispan_gen_free(g); return rc; }
+    {   // core; the planted SCCs tile the block from b_scc
+        PlantedInfo *pi = new PlantedInfo();
+        pi->perm = P.perm;
+        pi->n = n;
+        pi->n_core = P.n_core;
+        pi->block_lo = P.b_scc;
+        pi->bnd = off;
+        g->planted = pi;
+    }
     *out = g;
     return 0;
 }
@@ -901,8 +973,31 @@ int ispan_gen_extract(const ispan_gen_graph *g, int64_t vlo, int64_t vhi, void *
     return 0;
 }
 
+int ispan_gen_planted_labels(const ispan_gen_graph *g, int32_t *labels) {
+    if (!g || !labels) return -1;
+    if (!g->planted) return -4;
+    const PlantedInfo &pi = *g->planted;
+    if (cudaSetDevice(g->device) != cudaSuccess) return -3;
+    const int64_t nb = (int64_t)pi.bnd.size() - 1;
+    int64_t *d_bnd = nullptr;
+    int32_t *gmin = nullptr;
+    GK(cudaMalloc(&d_bnd, pi.bnd.size() * 8));
+    GK(cudaMalloc(&gmin, (nb + 1) * 4));
+    GK(cudaMemcpy(d_bnd, pi.bnd.data(), pi.bnd.size() * 8, cudaMemcpyHostToDevice));
+    GK(cudaMemset(gmin, 0x7f, (nb + 1) * 4));
+    k_planted_min<<<148 * 16, 256>>>(pi.perm, pi.n, pi.n_core, pi.block_lo, d_bnd, nb, gmin);
+    GK(cudaGetLastError());
+    k_planted_label<<<148 * 16, 256>>>(pi.perm, pi.n, pi.n_core, pi.block_lo, d_bnd, nb, gmin, labels);
+    GK(cudaGetLastError());
+    GK(cudaDeviceSynchronize());
+    cudaFree(d_bnd);
+    cudaFree(gmin);
+    return 0;
+}
+
 int ispan_gen_free(ispan_gen_graph *g) {
     if (!g) return 0;
+    delete g->planted;
     cudaSetDevice(g->device);
     cudaFree(g->fw_beg);
     cudaFree(g->bw_beg);

@@ -85,6 +85,9 @@ struct ispan_ctx {
     int64_t *h_vbeb = nullptr;                     // pinned [2 * (pk_n + 1)]
     int64_t pk_n = 0;
     std::vector<void *> pk_owned;
+    std::vector<int64_t> pk_vbase;  // segmentation of the packed union
+    int64_t pk_cur_n = 0, pk_Et = 0;
+    bool pk_ready = false;          // a packed union waits for its run
     int32_t *qv[2] = {nullptr, nullptr};
     int64_t *qe[2] = {nullptr, nullptr};
     int32_t *qchunk[2] = {nullptr, nullptr};
@@ -723,13 +726,14 @@ static int pk_reserve(ispan_ctx *c, int64_t n) {
     return ISPAN_OK;
 }
 
-static int run_graphs(ispan_ctx *c, const ispan_csr *gs, int32_t n, int32_t *const *labels_out,
-                      const ispan_params *p, ispan_stats *st) {
+// phase 1 of ispan_scc_run_graphs: the union of gs in the context's union
+// buffers, checked; the segmentation is kept for phase 2
+static int pack_graphs(ispan_ctx *c, const ispan_csr *gs, int32_t n) {
+    c->pk_ready = false;
     int64_t Vt = 0, Et = 0;
     for (int32_t i = 0; i < n; ++i) {
         int rc = check_csr(&gs[i]);
         if (rc) return rc;
-        if (gs[i].V > 0 && !labels_out[i]) return ISPAN_ERR_ARG;
         Vt += gs[i].V;
         Et += gs[i].E;
     }
@@ -804,7 +808,25 @@ static int run_graphs(ispan_ctx *c, const ispan_csr *gs, int32_t n, int32_t *con
     CK(cudaMemcpyAsync(c->h_err, c->err, 4 * sizeof(int), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     if (c->h_err[1]) return ISPAN_ERR_ARG;
-    std::vector<int64_t> vbase(hvb, hvb + n + 1);
+    c->pk_vbase.assign(hvb, hvb + n + 1);
+    c->pk_cur_n = n;
+    c->pk_Et = Et;
+    c->pk_ready = true;
+    return ISPAN_OK;
+}
+
+// phase 2: the pipeline over the packed union, then every graph's labels
+static int run_packed(ispan_ctx *c, const ispan_csr *gs, int32_t n, int32_t *const *labels_out,
+                      const ispan_params *p, ispan_stats *st) {
+    if (!c->pk_ready || c->pk_cur_n != n) return ISPAN_ERR_ARG;
+    for (int32_t i = 0; i < n; ++i)
+        if (gs[i].V != c->pk_vbase[i + 1] - c->pk_vbase[i] || (gs[i].V > 0 && !labels_out[i])) return ISPAN_ERR_ARG;
+    c->pk_ready = false;  // the union is consumed (labels overwrite the scratch)
+    cudaStream_t s = c->stream;
+    const std::vector<int64_t> vbase = c->pk_vbase;
+    const int64_t Vt = vbase[n], Et = c->pk_Et;
+    const int gv = (int)std::min<int64_t>(Vt / kPackTile + 1, 8 * c->nsm);
+    int rc = 0;
     ispan_csr u;
     memset(&u, 0, sizeof u);
     u.V = Vt;
@@ -827,6 +849,14 @@ static int run_graphs(ispan_ctx *c, const ispan_csr *gs, int32_t n, int32_t *con
             CK(cudaMemcpyAsync(labels_out[i], c->label + vbase[i], (size_t)gs[i].V * 4, cudaMemcpyDefault, s));
     CK(cudaStreamSynchronize(s));
     return ISPAN_OK;
+}
+
+static int run_graphs(ispan_ctx *c, const ispan_csr *gs, int32_t n, int32_t *const *labels_out,
+                      const ispan_params *p, ispan_stats *st) {
+    for (int32_t i = 0; i < n; ++i)
+        if (gs[i].V > 0 && !labels_out[i]) return ISPAN_ERR_ARG;
+    int rc = pack_graphs(c, gs, n);
+    return rc ? rc : run_packed(c, gs, n, labels_out, p, st);
 }
 
 extern "C" {
@@ -945,6 +975,21 @@ int ispan_scc_run_graphs(ispan_ctx *c, const ispan_csr *gs, int32_t n, int32_t *
     std::lock_guard<std::mutex> lock(c->mu);
     if (cudaSetDevice(c->device) != cudaSuccess) return ISPAN_ERR_CUDA;
     return run_graphs(c, gs, n, labels_out, p, st);
+}
+
+int ispan_graphs_pack(ispan_ctx *c, const ispan_csr *gs, int32_t n) {
+    if (!c || !gs || n < 1) return ISPAN_ERR_ARG;
+    std::lock_guard<std::mutex> lock(c->mu);
+    if (cudaSetDevice(c->device) != cudaSuccess) return ISPAN_ERR_CUDA;
+    return pack_graphs(c, gs, n);
+}
+
+int ispan_graphs_run(ispan_ctx *c, const ispan_csr *gs, int32_t n, int32_t *const *labels_out,
+                     const ispan_params *p, ispan_stats *st) {
+    if (!c || !gs || n < 1 || !labels_out) return ISPAN_ERR_ARG;
+    std::lock_guard<std::mutex> lock(c->mu);
+    if (cudaSetDevice(c->device) != cudaSuccess) return ISPAN_ERR_CUDA;
+    return run_packed(c, gs, n, labels_out, p, st);
 }
 
 int ispan_ref_codes(ispan_ctx *c, int32_t *codes) {

@@ -1,7 +1,8 @@
 // server.cu -- served SCC detection: requests (one graph each) are queued,
 // gathered into batches while the device works on the previous batch
 // (continuous batching), and run as one disjoint union per batch through
-// ispan_scc_run_graphs.  Declared in include/ispan_b200.h (ispan_server_*).
+// the two phases of ispan_scc_run_graphs (ispan_graphs_pack, then
+// ispan_graphs_run).  Declared in include/ispan_b200.h (ispan_server_*).
 //
 // The reference has no serving mode: it runs one graph per process
 // (src/scc_main.cpp:41-47).  Results are those of ispan_scc_run on the graph
@@ -9,11 +10,13 @@
 // graph, every segment gets its own pivot), and labels are translated back to
 // each graph's local ids.
 //
-// Admission: the server holds one context and the union buffers, sized from
-// the configured device-memory budget; a request larger than one batch is
-// refused at submission (ISPAN_ERR_CAPACITY), and the queue may be bounded
+// Admission: the budget is split between the batch slots, each a context
+// plus its union buffers; a request larger than one batch is refused at
+// submission (ISPAN_ERR_CAPACITY), and the queue may be bounded
 // (ISPAN_ERR_BUSY).  Requests run in arrival order; a batch takes requests
-// from the head of the queue while they fit.
+// from the head of the queue while they fit.  While one slot's batch runs,
+// another slot packs the next batch (host copies and the pack kernels on its
+// own stream), so arrivals join the device work as soon as a slot frees.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -53,8 +56,8 @@ int64_t server_bytes(int64_t V, int64_t E, int64_t n) {
 
 struct ispan_server {
     ispan_server_config cfg;
-    ispan_ctx *ctx = nullptr;
-    int64_t capV = 0, capE = 0;
+    std::vector<ispan_ctx *> ctx;   // one per batch slot
+    int64_t capV = 0, capE = 0;     // per batch (one slot)
     int32_t capN = 0;
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
@@ -63,7 +66,9 @@ struct ispan_server {
     int64_t next_ticket = 1, next_batch = 0;
     int64_t n_batches = 0, n_graphs = 0, n_vertices = 0, n_edges = 0, busy_ns = 0;
     bool stop = false;
-    std::thread worker;
+    bool device_busy = false;       // a slot's pipeline is on the device
+    std::mutex dev_mu;              // one pipeline on the device at a time
+    std::vector<std::thread> workers;
 
     bool batch_full() const {
         int64_t v = 0, e = 0, k = 0;
@@ -77,7 +82,26 @@ struct ispan_server {
         return false;
     }
 
-    void run_batch(std::vector<int64_t> &take) {
+    // pack on this slot's context (overlapping another slot's run), then run
+    // when the device is free
+    int pack_run(ispan_ctx *c, std::vector<ispan_csr> &gs, std::vector<int32_t *> &labs) {
+        int rc = ispan_graphs_pack(c, gs.data(), (int32_t)gs.size());
+        if (rc) return rc;
+        std::lock_guard<std::mutex> dev(dev_mu);
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            device_busy = true;
+        }
+        rc = ispan_graphs_run(c, gs.data(), (int32_t)gs.size(), labs.data(), &cfg.params, nullptr);
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            device_busy = false;
+        }
+        cv_work.notify_all();  // an idle device lets a waiting slot take a batch
+        return rc;
+    }
+
+    void run_batch(ispan_ctx *c, std::vector<int64_t> &take) {
         std::vector<ispan_csr> gs;
         std::vector<int32_t *> labs;
         {
@@ -90,12 +114,15 @@ struct ispan_server {
         }
         const int64_t t0 = now_ns();
         std::vector<int> rcs(take.size(), 0);
-        int rc = ispan_scc_run_graphs(ctx, gs.data(), (int32_t)gs.size(), labs.data(), &cfg.params, nullptr);
+        int rc = pack_run(c, gs, labs);
         if (rc == ISPAN_ERR_ARG && gs.size() > 1) {
             // a malformed graph fails the whole union: run each alone so only
             // that request reports the error
-            for (size_t i = 0; i < gs.size(); ++i)
-                rcs[i] = ispan_scc_run_graphs(ctx, &gs[i], 1, &labs[i], &cfg.params, nullptr);
+            for (size_t i = 0; i < gs.size(); ++i) {
+                std::vector<ispan_csr> g1(1, gs[i]);
+                std::vector<int32_t *> l1(1, labs[i]);
+                rcs[i] = pack_run(c, g1, l1);
+            }
         } else {
             std::fill(rcs.begin(), rcs.end(), rc);
         }
@@ -120,12 +147,15 @@ struct ispan_server {
         cv_done.notify_all();
     }
 
-    void loop() {
+    // A slot takes a batch when the device is idle (latency) or a full batch
+    // is queued (throughput: it packs while the running batch computes).
+    void loop(int slot) {
+        ispan_ctx *c = ctx[slot];
         for (;;) {
             std::vector<int64_t> take;
             {
                 std::unique_lock<std::mutex> lk(mu);
-                cv_work.wait(lk, [&] { return stop || !pending.empty(); });
+                cv_work.wait(lk, [&] { return stop || (!pending.empty() && (!device_busy || batch_full())); });
                 if (stop && pending.empty()) return;
                 if (cfg.max_wait_us > 0 && !stop) {
                     // let a partial batch fill for a bounded time
@@ -142,7 +172,7 @@ struct ispan_server {
                     pending.pop_front();
                 }
             }
-            if (!take.empty()) run_batch(take);
+            if (!take.empty()) run_batch(c, take);
         }
     }
 };
@@ -155,20 +185,22 @@ int ispan_server_create(const ispan_server_config *cfg, ispan_server **out) {
     ispan_server *s = new ispan_server();
     s->cfg = *cfg;
     const int64_t budget = cfg->hbm_budget_bytes > 0 ? cfg->hbm_budget_bytes : (64ll << 30);
+    const int nslots = cfg->n_slots > 0 ? cfg->n_slots : 2;
+    const int64_t share = budget / nslots;
     s->capN = cfg->max_batch_graphs > 0 ? cfg->max_batch_graphs : 4096;
     if (cfg->max_batch_V > 0 && cfg->max_batch_E >= 0) {
         s->capV = cfg->max_batch_V;
         s->capE = cfg->max_batch_E;
-        if (server_bytes(s->capV, s->capE, s->capN) > budget) {
+        if (server_bytes(s->capV, s->capE, s->capN) > share) {
             delete s;
             return ISPAN_ERR_NOMEM;
         }
     } else {
-        // the largest batch at 16 edges per vertex that fits the budget
+        // the largest batch at 16 edges per vertex that fits a slot's share
         int64_t lo = 0, hi = (int64_t)INT32_MAX - 64;
         while (lo < hi) {
             int64_t mid = (lo + hi + 1) / 2;
-            if (server_bytes(mid, 16 * mid, s->capN) <= budget) lo = mid; else hi = mid - 1;
+            if (server_bytes(mid, 16 * mid, s->capN) <= share) lo = mid; else hi = mid - 1;
         }
         if (lo < 1024) {
             delete s;
@@ -177,12 +209,17 @@ int ispan_server_create(const ispan_server_config *cfg, ispan_server **out) {
         s->capV = lo;
         s->capE = 16 * lo;
     }
-    int rc = ispan_ctx_create(cfg->device, s->capV, s->capE, &s->ctx);
-    if (rc) {
-        delete s;
-        return rc;
+    for (int k = 0; k < nslots; ++k) {
+        ispan_ctx *c = nullptr;
+        int rc = ispan_ctx_create(cfg->device, s->capV, s->capE, &c);
+        if (rc) {
+            for (ispan_ctx *d : s->ctx) ispan_ctx_destroy(d);
+            delete s;
+            return rc;
+        }
+        s->ctx.push_back(c);
     }
-    s->worker = std::thread([s] { s->loop(); });
+    for (int k = 0; k < nslots; ++k) s->workers.emplace_back([s, k] { s->loop(k); });
     *out = s;
     return ISPAN_OK;
 }
@@ -264,8 +301,9 @@ int ispan_server_destroy(ispan_server *s) {
         s->stop = true;
     }
     s->cv_work.notify_all();
-    if (s->worker.joinable()) s->worker.join();  // queued requests are served first
-    ispan_ctx_destroy(s->ctx);
+    for (std::thread &t : s->workers)  // queued requests are served first
+        if (t.joinable()) t.join();
+    for (ispan_ctx *c : s->ctx) ispan_ctx_destroy(c);
     delete s;
     return ISPAN_OK;
 }

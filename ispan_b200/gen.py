@@ -33,6 +33,7 @@ def lib():
         L.ispan_gen_batch.argtypes = [C.c_int, I32, I64, I64, I32, I32, I32, C.c_uint64, P, C.POINTER(P)]
         L.ispan_gen_info.argtypes = [P, C.POINTER(I64), C.POINTER(I64)]
         L.ispan_gen_copy.argtypes = [P, P, P, P, P, I32, I32]
+        L.ispan_gen_planted_labels.argtypes = [P, P]
         L.ispan_gen_device_ptrs.argtypes = [P, C.POINTER(P), C.POINTER(P), C.POINTER(P), C.POINTER(P)]
         L.ispan_gen_free.argtypes = [P]
         L.ispan_gen_extract.argtypes = [P, I64, I64, P, P, P, P, I32, C.POINTER(I64)]
@@ -63,6 +64,18 @@ class DeviceGraph:
         if rc:
             raise RuntimeError(f"ispan_gen_copy failed ({rc})")
         return CSR(self.V, self.E, fb, fa[:self.E], bb, ba[:self.E])
+
+    def planted_labels(self):
+        """The planted SCC partition as canonical labels (CUDA int32 tensor),
+        or None for generators without one (R-MAT, batch)."""
+        import torch
+        out = torch.empty(max(self.V, 1), dtype=torch.int32, device="cuda")
+        rc = lib().ispan_gen_planted_labels(self._h, out.data_ptr())
+        if rc == -4:
+            return None
+        if rc:
+            raise RuntimeError(f"ispan_gen_planted_labels failed ({rc})")
+        return out[:self.V]
 
     def to_pinned(self):
         """Copies in pinned host memory as CPU tensors (int64 offsets)."""

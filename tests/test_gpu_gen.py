@@ -72,3 +72,31 @@ def test_social_medium_repeated_runs_exact():
         for use_graph in (False, True, True, True):
             labels, st = ctx.run_csr(csr, use_graph=use_graph)
             assert np.array_equal(labels, exact)
+
+
+@pytest.mark.parametrize("kind,scale,seed", [("social", 0.005, 3), ("web", 0.004, 2)])
+def test_planted_partition_is_exact(kind, scale, seed):
+    """The generators' planted partition equals the exact SCC partition
+    (pins it as a full-size reference for the tests below)."""
+    g = getattr(gen, kind)(seed=seed, scale=scale)
+    planted = g.planted_labels().cpu().numpy()
+    exact = oracle.tarjan(g.to_host(np.int64))
+    assert np.array_equal(planted, exact)
+
+
+@pytest.mark.parametrize("kind,scale", [("social", 1.0), ("web", 0.2)])
+def test_large_graph_labels_equal_planted_partition(kind, scale):
+    """Full-size social graph (41.6 M vertices, 1.47 B edges) and a 140 M-vertex
+    web graph: every label equals the planted partition's, compared on the
+    device."""
+    import torch
+    g = getattr(gen, kind)(seed=1, scale=scale)
+    with Context(g.V, g.E) as ctx:
+        lab = torch.empty(g.V, dtype=torch.int32, device="cuda")
+        fb, fa, bb, ba = g.ptrs
+        _, st = ctx.run_raw(g.V, g.E, fb, fa, bb, ba, 8, lab)
+        planted = g.planted_labels()
+        assert int((lab != planted).sum()) == 0
+        n_scc = int((planted == torch.arange(g.V, dtype=torch.int32, device="cuda")).sum())
+        assert st["scc_count"] == n_scc
+    g.free()
