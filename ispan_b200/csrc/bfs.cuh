@@ -325,7 +325,10 @@ __device__ __forceinline__ void q_append_one(int32_t v, int64_t deg, int32_t *qv
 struct AsyncSmem {
     int32_t lq[2][kLQ];
     int cnt[2];
+    int flush;  // hand the local frontier back to the grid at the next level
 };
+
+constexpr int kAsyncFlush = kLQ / 2;  // a CTA's local frontier above this is work for the whole grid
 
 // Asynchronous top-down round (the GPU form of the reference's per-thread
 // ring-buffer mode, src/fw_bw.h:506-544).  Each CTA takes a slice of the
@@ -351,13 +354,15 @@ __device__ __forceinline__ void async_round(const Run<OffT> &r, const BfsDir<Off
         const int n0 = (int)min((int64_t)kLQ, s1 - bs);
         __syncthreads();
         for (int i = tid; i < n0; i += kBlock) sm.lq[0][i] = __ldcg(qv + bs + i);
-        if (tid == 0) { sm.cnt[0] = n0; sm.cnt[1] = 0; }
+        if (tid == 0) { sm.cnt[0] = n0; sm.cnt[1] = 0; sm.flush = 0; }
         __syncthreads();
         int c = 0;
         for (int it = 0; it < kAsyncMaxLevels; ++it) {
             const int n = sm.cnt[c];
             if (n == 0) break;
-            const bool last = it == kAsyncMaxLevels - 1;
+            // a frontier that widened (here, or grid-wide in the global queue)
+            // goes back to the edge-balanced top-down kernel
+            const bool last = it == kAsyncMaxLevels - 1 || sm.flush;
             for (int i = tid; i < n; i += kBlock) {
                 const int32_t v = sm.lq[c][i];
                 const int64_t x0 = ld_off(d.xbeg, v), x1 = ld_off(d.xbeg, v + 1);
@@ -401,8 +406,11 @@ __device__ __forceinline__ void async_round(const Run<OffT> &r, const BfsDir<Off
             if (tid == 0) {
                 sm.cnt[c ^ 1] = min(sm.cnt[c ^ 1], kLQ);  // claims beyond the capacity went global
                 sm.cnt[c] = 0;
+                const int64_t global_q = (int64_t)(__ldcg(pk_next) & kCountMask);
+                sm.flush = sm.cnt[c ^ 1] > kAsyncFlush || global_q > r.async_v;
             }
             __syncthreads();
+            if (last) break;  // this level only handed vertices on
             c ^= 1;
         }
     }
