@@ -358,7 +358,10 @@ def bench_batch(args, ws, rank, local):
     ctx = Context(g.V, g.E)
     ctx.set_stream(stream)
     labels = torch.empty(g.V, dtype=torch.int32, device="cuda")
-    run = lambda: ctx.run_raw(g.V, g.E, fwb, fwa, bwb, bwa, 8, labels, vbase=vb, stage_times=True)  # noqa: E731
+    from ispan_b200 import autotune
+    tp = autotune.apply(ctx, g.V, g.E, nseg)
+    tun = dict(alpha=tp["alpha"], beta=tp["beta"], gamma=tp["gamma"])
+    run = lambda: ctx.run_raw(g.V, g.E, fwb, fwa, bwb, bwa, 8, labels, vbase=vb, stage_times=True, **tun)  # noqa: E731
     for _ in range(args.warmup):
         run()
     torch.cuda.synchronize()
@@ -390,10 +393,12 @@ def bench_batch(args, ws, rank, local):
             plain = Context(maxv, int(fa.numel()) * 2)
             plain.set_stream(stream)
         out = torch.empty(fb.numel() - 1, dtype=torch.int32, device="cuda")
-        plain.run(fb, fa, bb, ba, labels_out=out)  # warm (captures the graph for this shape)
+        tpp = autotune.apply(plain, int(fb.numel()) - 1, int(fa.numel()))  # tuned like the batch
+        tpl = dict(alpha=tpp["alpha"], beta=tpp["beta"], gamma=tpp["gamma"])
+        plain.run(fb, fa, bb, ba, labels_out=out, **tpl)  # warm (captures the graph for this shape)
         a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a0.record(stream)
-        plain.run(fb, fa, bb, ba, labels_out=out)
+        plain.run(fb, fa, bb, ba, labels_out=out, **tpl)
         a1.record(stream)
         torch.cuda.synchronize()
         per_ms.append(a0.elapsed_time(a1))
@@ -623,7 +628,10 @@ def main():
     ctx.set_stream(stream)
     fb, fa, bb, ba = g.ptrs  # the generator's device arrays, no copy
     labels = torch.empty(g.V, dtype=torch.int32, device="cuda")
-    run = lambda: ctx.run_raw(g.V, g.E, fb, fa, bb, ba, 8, labels, stage_times=True)  # noqa: E731
+    from ispan_b200 import autotune
+    tp = autotune.apply(ctx, g.V, g.E)  # the tuned launch parameters of this graph's shape class
+    tun = dict(alpha=tp["alpha"], beta=tp["beta"], gamma=tp["gamma"])
+    run = lambda: ctx.run_raw(g.V, g.E, fb, fa, bb, ba, 8, labels, stage_times=True, **tun)  # noqa: E731
     for _ in range(args.warmup):
         _, st = run()
     torch.cuda.synchronize()
@@ -651,7 +659,7 @@ def main():
 
     # roofline of the dominant kernel (the longer of the FW and BW searches);
     # the degree sums of the reached sets come from one extra, untimed run
-    _, st_x = ctx.run_raw(g.V, g.E, fb, fa, bb, ba, 8, labels, exact_stats=True)
+    _, st_x = ctx.run_raw(g.V, g.E, fb, fa, bb, ba, 8, labels, exact_stats=True, **tun)
     st = dict(st, fw_edges=st_x["fw_edges"], bw_edges=st_x["bw_edges"])
     fw_b, bw_b = alg_bytes(st)
     fw_ms = statistics.mean(s["stage_ms"][7] for s in stages)
@@ -691,13 +699,13 @@ def main():
         np_args = [t.numpy() for t in (hfb, hfa, hbb, hba)]
         g.free()  # the upload buffers take the generator's place on the device
         torch.cuda.empty_cache()
-        ctx.run(*np_args, V=g.V, labels_out=hlab.numpy())  # warm (allocates the upload buffers)
+        ctx.run(*np_args, V=g.V, labels_out=hlab.numpy(), **tun)  # warm (allocates the upload buffers)
         barrier(ws)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         for _ in range(args.e2e_steps):
-            ctx.run(*np_args, V=g.V, labels_out=hlab.numpy())
+            ctx.run(*np_args, V=g.V, labels_out=hlab.numpy(), **tun)
         e1.record(stream)
         torch.cuda.synchronize()
         e2e_ms = max_over_ranks(e0.elapsed_time(e1), ws) / args.e2e_steps
@@ -710,7 +718,8 @@ def main():
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "int32", "data": "synthetic",
             "config": dict(desc, parallelism="replicas" if ws > 1 else "single-gpu",
-                           l2="inputs larger than L2 (CSR resident in HBM)"),
+                           l2="inputs larger than L2 (CSR resident in HBM)",
+                           tuning=dict(tp, shape_class=autotune.shape_class(g.V, g.E))),
             "e2e": e2e, "gpu_launches": KERNELS_PER_STEP * args.steps, "roofline": roof, "cpu_baseline": cpu,
             "clocks": clk,
             "stage_ms": {"trim": stage_mean[0], "elephant": stage_mean[1], "mice": stage_mean[2],
