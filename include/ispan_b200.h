@@ -202,6 +202,17 @@ int ispan_server_counters(ispan_server *s, int64_t *out, int32_t n);
 /* Serves what is queued, then stops the worker and frees the device memory. */
 int ispan_server_destroy(ispan_server *s);
 
+/* Condensation: the DAG of the SCCs of a device-resident graph g (only its
+ * forward CSR is read) given device labels[V] from a run on it.  Components
+ * are named by their canonical labels; pairs_out (host or device, up to cap
+ * entries) receives each distinct crossing pair as (source label << 32 |
+ * target label), sorted; *n_pairs gets the number of distinct pairs (call
+ * with cap 0 to size the buffer).  Allocates temporary device memory.  The
+ * reference stops at class counts (src/load_print.cpp:24-60); this is the
+ * step after the path. */
+int ispan_condense(const ispan_csr *g, const int32_t *labels, uint64_t *pairs_out, int64_t cap,
+                   int64_t *n_pairs, void *stream);
+
 /* Largest graph (vertices) that ispan_scc_small_noalloc accepts. */
 #define ISPAN_NOALLOC_MAX_V 65536
 

@@ -24,7 +24,7 @@ from . import _lib
 from ._lib import IspanError, check
 from .graphs import CSR, read_bin
 
-__all__ = ["Context", "Server", "graph", "graph_load", "scc_detection", "get_scc_result", "print_time_result",
+__all__ = ["Context", "Server", "condensation", "graph", "graph_load", "scc_detection", "get_scc_result", "print_time_result",
            "IspanError", "CSR", "scc"]
 
 REFERENCE_DEFAULTS = dict(alpha=30, beta=200, gamma=10, theta=0.1)  # src/bash_one.sh:4
@@ -289,6 +289,23 @@ class Server:
 
     def __exit__(self, *a):
         self.close()
+
+
+def condensation(fw_beg, fw_adj, labels, stream=None) -> np.ndarray:
+    """The SCC DAG of a device graph (torch CUDA tensors: forward offsets and
+    adjacency) given its device labels: an (n, 2) int64 array of distinct
+    (source label, target label) pairs, sorted."""
+    V = fw_beg.numel() - 1
+    g = _lib.Csr(V, fw_adj.numel(), _ptr(fw_beg), _ptr(fw_beg), _ptr(fw_adj), _ptr(fw_adj),
+                 fw_beg.element_size(), 1)
+    n = C.c_int64()
+    h = C.c_void_p(0 if stream is None else int(getattr(stream, "cuda_stream", stream)))
+    check(_lib.lib().ispan_condense(C.byref(g), C.c_void_p(_ptr(labels)), None, 0, C.byref(n), h), "ispan_condense")
+    out = np.empty(max(n.value, 1), np.uint64)
+    check(_lib.lib().ispan_condense(C.byref(g), C.c_void_p(_ptr(labels)), C.c_void_p(out.ctypes.data), n.value,
+                                    C.byref(n), h), "ispan_condense")
+    out = out[:n.value]
+    return np.stack([(out >> np.uint64(32)).astype(np.int64), (out & np.uint64(0xffffffff)).astype(np.int64)], 1)
 
 
 def scc(csr: CSR, **kw):
