@@ -108,6 +108,8 @@ typedef struct {
     int64_t async_e;          /* ... and this many frontier edges (262144) */
     int32_t async_deg;        /* an asynchronous CTA expands vertices up to this degree itself (16) */
     int32_t bfs_ctas_per_sm;  /* CTAs per SM of the persistent searches, at most the occupancy limit (2) */
+    int32_t color_levels;     /* local levels a CTA works per grid round when colouring large WCCs (32) */
+    int32_t reserved;
 } ispan_tuning;
 
 /* NULL restores the defaults; the next run re-captures its CUDA graph. */

@@ -4,12 +4,15 @@ Tuned: the push/pull switch of the reachability searches (alpha, beta, gamma:
 the reference's own knobs, src/fw_bw.h:576-624, whose defaults 30/200/10 come
 from src/bash_one.sh:4), the frontier sizes and vertex degree below which a
 search runs asynchronously inside CTAs (async_v, async_e, async_deg), and
-the CTAs per SM of the persistent searches (bfs_ctas_per_sm).  None of them
+the CTAs per SM of the persistent searches (bfs_ctas_per_sm), and the local
+levels a CTA works per grid round when colouring large WCCs (color_levels:
+fewer levels balance the CTAs, more save grid barriers).  None of them
 changes a label; they only move time between stages.
 
 Method: coordinate descent from the defaults over a small grid per
-parameter, two passes, each candidate timed as the median of several runs of
-the whole pipeline on the device (CUDA events inside the captured graph).
+parameter, two passes, each candidate timed as the median of several runs on
+the device (CUDA events inside the captured graph) of the stages the
+tunables act on (trim and elephant).
 The winners are stored per shape class in ``tuning_table.json`` beside this
 file; :func:`apply` looks a graph's class up and sets the context.
 
@@ -26,7 +29,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 TABLE = os.path.join(HERE, "tuning_table.json")
 
 DEFAULTS = {"alpha": 30, "beta": 200, "gamma": 10, "async_v": 65536, "async_e": 262144, "async_deg": 16,
-            "bfs_ctas_per_sm": 0}
+            "bfs_ctas_per_sm": 0, "color_levels": 32}
 SPACE = {
     "alpha": [5, 10, 30, 100, 300],
     "beta": [50, 200, 1000, 4000],
@@ -35,6 +38,7 @@ SPACE = {
     "async_e": [16384, 65536, 262144, 1048576],
     "async_deg": [4, 16, 64],
     "bfs_ctas_per_sm": [1, 0],
+    "color_levels": [4, 8, 16, 32, 64, 256],
 }
 
 
@@ -57,7 +61,7 @@ def load_table(path: str = TABLE) -> dict:
 def lookup(V: int, E: int, nseg: int = 1, path: str = TABLE) -> dict | None:
     """Tuned parameters of the graph's class, or None if the class was never tuned."""
     ent = load_table(path)["classes"].get(shape_class(V, E, nseg))
-    return None if ent is None else {k: ent["params"][k] for k in DEFAULTS}
+    return None if ent is None else {k: ent["params"].get(k, DEFAULTS[k]) for k in DEFAULTS}
 
 
 def apply(ctx, V: int, E: int, nseg: int = 1, path: str = TABLE) -> dict:
@@ -67,15 +71,21 @@ def apply(ctx, V: int, E: int, nseg: int = 1, path: str = TABLE) -> dict:
     t = lookup(V, E, nseg, path)
     if t:
         p.update(t)
-    ctx.set_tuning(p["async_v"], p["async_e"], p["async_deg"], p["bfs_ctas_per_sm"])
+    ctx.set_tuning(p["async_v"], p["async_e"], p["async_deg"], p["bfs_ctas_per_sm"], p["color_levels"])
     return p
 
 
+def tuned_ms(stage_ms) -> float:
+    """The time the tunables act on: the trim, elephant and mice stages
+    (reference slots 0, 1 and 2; their sum is the pipeline time)."""
+    return stage_ms[0] + stage_ms[1] + stage_ms[2]
+
+
 def measure(ctx, run, p: dict, reps: int = 5) -> float:
-    """Median pipeline time (ms, device events) of run(alpha, beta, gamma) under p."""
-    ctx.set_tuning(p["async_v"], p["async_e"], p["async_deg"], p["bfs_ctas_per_sm"])
+    """Median trim + elephant + mice time (ms, device events) of run(alpha, beta, gamma) under p."""
+    ctx.set_tuning(p["async_v"], p["async_e"], p["async_deg"], p["bfs_ctas_per_sm"], p["color_levels"])
     run(p["alpha"], p["beta"], p["gamma"])  # capture the graph for these values
-    ts = [run(p["alpha"], p["beta"], p["gamma"])["stage_ms"][3] for _ in range(reps)]
+    ts = [tuned_ms(run(p["alpha"], p["beta"], p["gamma"])["stage_ms"]) for _ in range(reps)]
     return statistics.median(ts)
 
 

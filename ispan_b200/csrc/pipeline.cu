@@ -113,7 +113,7 @@ struct ispan_ctx {
     unsigned long long *h_counters = nullptr;  // pinned
     int *h_err = nullptr;
 
-    ispan_tuning tuning = {0, 0, 0, 0};
+    ispan_tuning tuning = {0, 0, 0, 0, 0, 0};
 
     // launch geometry
     int g_stream = 0;           // grid for plain grid-stride kernels
@@ -280,6 +280,7 @@ static void fill_run(ispan_ctx *c, Run<OffT> &r, Ext<OffT> &x, int64_t V, int64_
     r.async_v = c->tuning.async_v > 0 ? c->tuning.async_v : kAsyncV;
     r.async_e = c->tuning.async_e > 0 ? c->tuning.async_e : kAsyncE;
     r.async_deg = c->tuning.async_deg > 0 ? c->tuning.async_deg : kAsyncDeg;
+    r.color_levels = c->tuning.color_levels > 0 ? c->tuning.color_levels : kCLevels;
     x.ctl = c->ctlblk + kCtlX;
     x.roots = c->roots;
     x.small = c->small;
@@ -936,10 +937,10 @@ int ispan_ctx_set_stream(ispan_ctx *c, void *stream) {
 
 int ispan_ctx_set_tuning(ispan_ctx *c, const ispan_tuning *t) {
     if (!c) return ISPAN_ERR_ARG;
-    if (t && (t->async_v < 0 || t->async_e < 0 || t->async_deg < 0 || t->bfs_ctas_per_sm < 0))
+    if (t && (t->async_v < 0 || t->async_e < 0 || t->async_deg < 0 || t->bfs_ctas_per_sm < 0 || t->color_levels < 0))
         return ISPAN_ERR_ARG;
     std::lock_guard<std::mutex> lock(c->mu);
-    c->tuning = t ? *t : ispan_tuning{0, 0, 0, 0};
+    c->tuning = t ? *t : ispan_tuning{0, 0, 0, 0, 0, 0};
     c->g_coop_w = 0;  // recompute the persistent grids
     if (c->gexec) {   // the captured graph holds the old values
         cudaGraphExecDestroy(c->gexec);
@@ -955,6 +956,8 @@ int ispan_ctx_get_tuning(ispan_ctx *c, ispan_tuning *t) {
     t->async_e = c->tuning.async_e > 0 ? c->tuning.async_e : kAsyncE;
     t->async_deg = c->tuning.async_deg > 0 ? c->tuning.async_deg : kAsyncDeg;
     t->bfs_ctas_per_sm = c->tuning.bfs_ctas_per_sm;
+    t->color_levels = c->tuning.color_levels > 0 ? c->tuning.color_levels : kCLevels;
+    t->reserved = 0;
     return ISPAN_OK;
 }
 

@@ -895,10 +895,13 @@ __device__ __forceinline__ uint32_t prio_of(uint32_t v) {
 }
 
 constexpr int kCLQ = 2048;
+constexpr int kCLevels = 32;  // default of Run::color_levels: local levels a CTA works per grid round
 struct ColorSmem {
     int32_t lq[2][kCLQ];
     int cnt[2];
     int take;  // slice entries joining the next level
+    int rem;   // handed back: the frontier entries and the unread slice
+    unsigned long long base;
 };
 
 // One asynchronous round over the global queue q_in[0..n_in).  KIND 0
@@ -979,6 +982,22 @@ __device__ __forceinline__ void color_async_round(const Run<OffT> &r, const Ext<
                 }
             }
             __syncthreads();
+            if (it + 1 >= r.color_levels) {
+                // Enough local levels this grid round: the frontier and the
+                // unread rest of the slice go back to the grid queue, so no
+                // CTA keeps the others waiting at the grid barrier; the next
+                // round spreads them over all CTAs.
+                const int m = min(sm.cnt[c ^ 1], kCLQ);
+                const int64_t rest = s1 - next_in;
+                if (tid == 0) sm.base = atomicAdd(n_out, (unsigned long long)(m + rest));
+                __syncthreads();
+                const unsigned long long b0 = sm.base;
+                for (int i = tid; i < m; i += kBlock)
+                    if (VOK((long long)(b0 + i), 18)) q_out[b0 + i] = sm.lq[c ^ 1][i];
+                for (int64_t i = tid; i < rest; i += kBlock)
+                    if (VOK((long long)(b0 + m + i), 18)) q_out[b0 + m + i] = __ldcg(q_in + next_in + i);
+                break;
+            }
             if (tid == 0) {
                 const int m = min(sm.cnt[c ^ 1], kCLQ);
                 const int take = (int)min((int64_t)(kCLQ - m), s1 - next_in);

@@ -28,7 +28,8 @@ def test_lookup_and_apply(tmp_path):
     assert AT.lookup(41_652_231, 1_470_188_297, path=str(p)) is None
     ctx = FakeCtx()
     got = AT.apply(ctx, 65_536, 955_000, path=str(p))
-    assert got["alpha"] == 100 and ctx.calls == [(4096, AT.DEFAULTS["async_e"], AT.DEFAULTS["async_deg"], 1)]
+    assert got["alpha"] == 100 and ctx.calls == [(4096, AT.DEFAULTS["async_e"], AT.DEFAULTS["async_deg"], 1,
+                                                  AT.DEFAULTS["color_levels"])]
     ctx = FakeCtx()
     assert AT.apply(ctx, 10, 10, path=str(p)) == AT.DEFAULTS  # untuned class: defaults
 
@@ -45,7 +46,7 @@ def test_descent_keeps_only_clear_gains():
     def run(a, b, c):
         t = ctx.calls[-1]
         cost = 10.0 + (a != target["alpha"]) + (b != target["beta"]) + (t[2] != target["async_deg"])
-        return {"stage_ms": [0, 0, 0, cost]}
+        return {"stage_ms": [cost / 2, cost / 2, 0.0, cost]}
 
     best, ms, dms = AT.tune(ctx, run, passes=2, reps=1, log=lambda *_: None)
     assert (best["alpha"], best["beta"], best["async_deg"]) == (100, 1000, 64)
