@@ -51,6 +51,17 @@ int ispan_gen_web(int device, int64_t n, int64_t edges, double giant_frac, doubl
 int ispan_gen_batch(int device, int32_t nseg, int64_t vmin, int64_t vmax, int32_t ef_min, int32_t ef_max,
                     int32_t max_cycle, uint64_t seed, int64_t *vbase_out, ispan_gen_graph **out);
 
+/* CSR construction from an edge list (src[i] -> dst[i], i < m, ids in
+ * [0, V); host arrays, or device arrays when on_device != 0): both CSR
+ * directions, adjacency sorted, self-loops and duplicate edges dropped
+ * (neither changes the SCC partition).  The result is a handle like a
+ * generator's (copy, device pointers, free).  An id outside [0, V) returns -1.
+ * Replaces the reference's offline converter (graph_converter/
+ * txt_to_bin_fw_int.cpp, txt_to_bin_bw_int.cpp), which writes the same two
+ * CSR directions from a text edge list on the CPU. */
+int ispan_gen_from_edges(int device, int64_t V, const int32_t *src, const int32_t *dst, int64_t m,
+                         int32_t on_device, ispan_gen_graph **out);
+
 /* sizes of a generated graph */
 int ispan_gen_info(const ispan_gen_graph *g, int64_t *V, int64_t *E);
 

@@ -327,6 +327,17 @@ __global__ void k_flag_unique(const uint64_t *k, int64_t n, uint8_t *flag) {
     }
 }
 
+// user edge list -> sort keys (src << 32 | dst); ids outside [0, V) are reported
+__global__ void k_edge_keys(const int32_t *src, const int32_t *dst, int64_t m, int64_t V, uint64_t *keys,
+                            int *bad) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t s = src[i], d = dst[i];
+        const bool ok = s >= 0 && s < V && d >= 0 && d < V;
+        if (!ok) atomicOr(bad, 1);
+        keys[i] = ok ? ((uint64_t)(uint32_t)s << 32) | (uint32_t)d : 0ull;  // 0 -> 0 is a self-loop, dropped
+    }
+}
+
 // offsets from keys sorted by src: beg[v] = first index with src >= v
 __global__ void k_offsets(const uint64_t *k, int64_t n, int64_t V, int64_t *beg, int32_t *adj) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i <= n; i += (int64_t)gridDim.x * blockDim.x) {
@@ -970,6 +981,48 @@ int ispan_gen_extract(const ispan_gen_graph *g, int64_t vlo, int64_t vhi, void *
     if (bw_adj) k_extract_adj<<<148 * 4, 256>>>(g->bw_adj, b0, b1 - b0, vlo, bw_adj);
     GK(cudaGetLastError());
     GK(cudaDeviceSynchronize());
+    return 0;
+}
+
+int ispan_gen_from_edges(int device, int64_t V, const int32_t *src, const int32_t *dst, int64_t m,
+                         int32_t on_device, ispan_gen_graph **out) {
+    if (!out || V < 1 || V >= (1ll << 31) - 1 || m < 0 || (m > 0 && (!src || !dst))) return -1;
+    *out = nullptr;
+    if (cudaSetDevice(device) != cudaSuccess) return -3;
+    const int32_t *ds = src, *dd = dst;
+    int32_t *tmp = nullptr;
+    if (!on_device && m > 0) {  // stage host edges on the device
+        GK(cudaMalloc(&tmp, 2 * m * sizeof(int32_t)));
+        GK(cudaMemcpy(tmp, src, m * sizeof(int32_t), cudaMemcpyHostToDevice));
+        GK(cudaMemcpy(tmp + m, dst, m * sizeof(int32_t), cudaMemcpyHostToDevice));
+        ds = tmp;
+        dd = tmp + m;
+    }
+    uint64_t *ka = nullptr, *kb = nullptr;
+    int *bad = nullptr;
+    int h_bad = 0;
+    if (alloc_keys(m, &ka, &kb)) { cudaFree(tmp); return -2; }
+    GK(cudaMalloc(&bad, sizeof(int)));
+    GK(cudaMemset(bad, 0, sizeof(int)));
+    if (m > 0) {
+        k_edge_keys<<<148 * 16, 256>>>(ds, dd, m, V, ka, bad);
+        GK(cudaGetLastError());
+    }
+    GK(cudaMemcpy(&h_bad, bad, sizeof(int), cudaMemcpyDeviceToHost));
+    cudaFree(bad);
+    cudaFree(tmp);
+    if (h_bad) {  // an id outside [0, V)
+        cudaFree(ka);
+        cudaFree(kb);
+        return -1;
+    }
+    ispan_gen_graph *g = new ispan_gen_graph();
+    g->device = device;
+    int rc = build_csr(ka, kb, m, V, g);
+    cudaFree(ka);
+    cudaFree(kb);
+    if (rc) { ispan_gen_free(g); return rc; }
+    *out = g;
     return 0;
 }
 

@@ -34,6 +34,7 @@ def lib():
         L.ispan_gen_info.argtypes = [P, C.POINTER(I64), C.POINTER(I64)]
         L.ispan_gen_copy.argtypes = [P, P, P, P, P, I32, I32]
         L.ispan_gen_planted_labels.argtypes = [P, P]
+        L.ispan_gen_from_edges.argtypes = [C.c_int, I64, P, P, I64, I32, C.POINTER(P)]
         L.ispan_gen_device_ptrs.argtypes = [P, C.POINTER(P), C.POINTER(P), C.POINTER(P), C.POINTER(P)]
         L.ispan_gen_free.argtypes = [P]
         L.ispan_gen_extract.argtypes = [P, I64, I64, P, P, P, P, I32, C.POINTER(I64)]
@@ -179,6 +180,23 @@ def web(seed=1, scale=1.0, device=0, **kw) -> DeviceGraph:
     rc = lib().ispan_gen_web(device, p["n"], p["edges"], p["giant_frac"], p["trivial_frac"], p["min_scc"],
                              p["max_scc"], seed, C.byref(h))
     return _mk(rc, h, "ispan_gen_web")
+
+
+def from_edges(V: int, src, dst, device=0) -> DeviceGraph:
+    """Both CSR directions of an edge list on the GPU (numpy or CUDA int32
+    arrays); sorted, self-loops and duplicates dropped."""
+    import numpy as _np
+    on_dev = hasattr(src, "is_cuda") and src.is_cuda
+    if not on_dev:
+        src = _np.ascontiguousarray(src, _np.int32)
+        dst = _np.ascontiguousarray(dst, _np.int32)
+        ps, pd = src.ctypes.data, dst.ctypes.data
+        m = len(src)
+    else:
+        ps, pd, m = src.data_ptr(), dst.data_ptr(), src.numel()
+    h = C.c_void_p()
+    rc = lib().ispan_gen_from_edges(device, int(V), ps, pd, int(m), 1 if on_dev else 0, C.byref(h))
+    return _mk(rc, h, "ispan_gen_from_edges")
 
 
 def batch(nseg=4096, vmin=1000, vmax=1_000_000, ef_min=8, ef_max=32, max_cycle=1000, seed=1, device=0):

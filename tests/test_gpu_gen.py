@@ -100,3 +100,28 @@ def test_large_graph_labels_equal_planted_partition(kind, scale):
         n_scc = int((planted == torch.arange(g.V, dtype=torch.int32, device="cuda")).sum())
         assert st["scc_count"] == n_scc
     g.free()
+
+
+@pytest.mark.parametrize("on_device", [False, True])
+def test_csr_from_edge_list(on_device):
+    """GPU CSR construction from an edge list equals the host construction of
+    the deduplicated list (both directions, adjacency sorted); the SCC labels
+    of the raw list (duplicates and self-loops kept) are the same."""
+    import torch
+    rng = np.random.default_rng(11)
+    V, m = 3000, 20000
+    e = rng.integers(0, V, size=(m, 2))
+    e = np.concatenate([e, e[:500], np.stack([np.arange(50), np.arange(50)], 1)])  # duplicates, self-loops
+    src, dst = e[:, 0].astype(np.int32), e[:, 1].astype(np.int32)
+    if on_device:
+        g = gen.from_edges(V, torch.from_numpy(src).cuda(), torch.from_numpy(dst).cuda())
+    else:
+        g = gen.from_edges(V, src, dst)
+    got = g.to_host(np.int64)
+    want = G.from_edges(V, G.dedupe_edges(e), offset_dtype=np.int64)
+    for k in ("fw_beg", "fw_adj", "bw_beg", "bw_adj"):
+        assert np.array_equal(getattr(got, k), getattr(want, k)), k
+    assert np.array_equal(oracle.tarjan(got), oracle.tarjan(G.from_edges(V, e)))
+    g.free()
+    with pytest.raises(RuntimeError):
+        gen.from_edges(10, np.array([0, 11], np.int32), np.array([1, 2], np.int32))
