@@ -109,7 +109,7 @@ typedef struct {
     int32_t async_deg;        /* an asynchronous CTA expands vertices up to this degree itself (16) */
     int32_t bfs_ctas_per_sm;  /* CTAs per SM of the persistent searches, at most the occupancy limit (2) */
     int32_t color_levels;     /* local levels a CTA works per grid round when colouring large WCCs (32) */
-    int32_t reserved;
+    int32_t color_pivots;     /* about this many pivots in the first colouring round; doubles per round (1024) */
 } ispan_tuning;
 
 /* NULL restores the defaults; the next run re-captures its CUDA graph. */

@@ -78,17 +78,17 @@ class Context:
         return _lib.Csr(int(V), int(E), _ptr(fw_beg), _ptr(bw_beg), _ptr(fw_adj), _ptr(bw_adj), ob,
                         1 if on_device else 0)
 
-    def set_tuning(self, async_v=0, async_e=0, async_deg=0, bfs_ctas_per_sm=0, color_levels=0) -> None:
+    def set_tuning(self, async_v=0, async_e=0, async_deg=0, bfs_ctas_per_sm=0, color_levels=0,
+                   color_pivots=0) -> None:
         """Launch tunables (zero = default); see ispan_b200.autotune."""
-        t = _lib.Tuning(int(async_v), int(async_e), int(async_deg), int(bfs_ctas_per_sm), int(color_levels), 0)
+        t = _lib.Tuning(int(async_v), int(async_e), int(async_deg), int(bfs_ctas_per_sm), int(color_levels),
+                        int(color_pivots))
         check(_lib.lib().ispan_ctx_set_tuning(self._h, C.byref(t)), "ispan_ctx_set_tuning")
 
     def tuning(self) -> dict:
         t = _lib.Tuning()
         check(_lib.lib().ispan_ctx_get_tuning(self._h, C.byref(t)), "ispan_ctx_get_tuning")
-        d = t.as_dict()
-        d.pop("reserved", None)
-        return d
+        return t.as_dict()
 
     def run(self, fw_beg, fw_adj, bw_beg, bw_adj, V: int | None = None, labels_out=None,
             vbase=None, alpha=30, beta=200, gamma=10, theta=0.1, stage_times=False, use_graph=True,

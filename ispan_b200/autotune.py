@@ -6,7 +6,8 @@ from src/bash_one.sh:4), the frontier sizes and vertex degree below which a
 search runs asynchronously inside CTAs (async_v, async_e, async_deg), and
 the CTAs per SM of the persistent searches (bfs_ctas_per_sm), and the local
 levels a CTA works per grid round when colouring large WCCs (color_levels:
-fewer levels balance the CTAs, more save grid barriers).  None of them
+fewer levels balance the CTAs, more save grid barriers) and the pivots of its
+first round (color_pivots).  None of them
 changes a label; they only move time between stages.
 
 Method: coordinate descent from the defaults over a small grid per
@@ -29,7 +30,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 TABLE = os.path.join(HERE, "tuning_table.json")
 
 DEFAULTS = {"alpha": 30, "beta": 200, "gamma": 10, "async_v": 65536, "async_e": 262144, "async_deg": 16,
-            "bfs_ctas_per_sm": 0, "color_levels": 32}
+            "bfs_ctas_per_sm": 0, "color_levels": 32, "color_pivots": 1024}
 SPACE = {
     "alpha": [5, 10, 30, 100, 300],
     "beta": [50, 200, 1000, 4000],
@@ -39,6 +40,7 @@ SPACE = {
     "async_deg": [4, 16, 64],
     "bfs_ctas_per_sm": [1, 0],
     "color_levels": [4, 8, 16, 32, 64, 256],
+    "color_pivots": [256, 1024, 8192, 65536],
 }
 
 
@@ -71,7 +73,8 @@ def apply(ctx, V: int, E: int, nseg: int = 1, path: str = TABLE) -> dict:
     t = lookup(V, E, nseg, path)
     if t:
         p.update(t)
-    ctx.set_tuning(p["async_v"], p["async_e"], p["async_deg"], p["bfs_ctas_per_sm"], p["color_levels"])
+    ctx.set_tuning(p["async_v"], p["async_e"], p["async_deg"], p["bfs_ctas_per_sm"], p["color_levels"],
+                   p["color_pivots"])
     return p
 
 
@@ -83,7 +86,8 @@ def tuned_ms(stage_ms) -> float:
 
 def measure(ctx, run, p: dict, reps: int = 5) -> float:
     """Median trim + elephant + mice time (ms, device events) of run(alpha, beta, gamma) under p."""
-    ctx.set_tuning(p["async_v"], p["async_e"], p["async_deg"], p["bfs_ctas_per_sm"], p["color_levels"])
+    ctx.set_tuning(p["async_v"], p["async_e"], p["async_deg"], p["bfs_ctas_per_sm"], p["color_levels"],
+                   p["color_pivots"])
     run(p["alpha"], p["beta"], p["gamma"])  # capture the graph for these values
     ts = [tuned_ms(run(p["alpha"], p["beta"], p["gamma"])["stage_ms"]) for _ in range(reps)]
     return statistics.median(ts)

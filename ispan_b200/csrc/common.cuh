@@ -69,6 +69,7 @@ struct Run {
     int64_t async_v, async_e;     // a search goes asynchronous below these frontier sizes
     int32_t async_deg;            // degree up to which an asynchronous CTA expands a vertex itself
     int32_t color_levels;         // local levels a CTA works per grid round of the colouring searches
+    int32_t color_pivots;         // about this many pivots in the first colouring round
 };
 
 // statistics counters (indices into Run::counters)

@@ -281,6 +281,7 @@ static void fill_run(ispan_ctx *c, Run<OffT> &r, Ext<OffT> &x, int64_t V, int64_
     r.async_e = c->tuning.async_e > 0 ? c->tuning.async_e : kAsyncE;
     r.async_deg = c->tuning.async_deg > 0 ? c->tuning.async_deg : kAsyncDeg;
     r.color_levels = c->tuning.color_levels > 0 ? c->tuning.color_levels : kCLevels;
+    r.color_pivots = c->tuning.color_pivots > 0 ? c->tuning.color_pivots : kCPivots;
     x.ctl = c->ctlblk + kCtlX;
     x.roots = c->roots;
     x.small = c->small;
@@ -937,7 +938,8 @@ int ispan_ctx_set_stream(ispan_ctx *c, void *stream) {
 
 int ispan_ctx_set_tuning(ispan_ctx *c, const ispan_tuning *t) {
     if (!c) return ISPAN_ERR_ARG;
-    if (t && (t->async_v < 0 || t->async_e < 0 || t->async_deg < 0 || t->bfs_ctas_per_sm < 0 || t->color_levels < 0))
+    if (t && (t->async_v < 0 || t->async_e < 0 || t->async_deg < 0 || t->bfs_ctas_per_sm < 0 || t->color_levels < 0 ||
+              t->color_pivots < 0))
         return ISPAN_ERR_ARG;
     std::lock_guard<std::mutex> lock(c->mu);
     c->tuning = t ? *t : ispan_tuning{0, 0, 0, 0, 0, 0};
@@ -957,7 +959,7 @@ int ispan_ctx_get_tuning(ispan_ctx *c, ispan_tuning *t) {
     t->async_deg = c->tuning.async_deg > 0 ? c->tuning.async_deg : kAsyncDeg;
     t->bfs_ctas_per_sm = c->tuning.bfs_ctas_per_sm;
     t->color_levels = c->tuning.color_levels > 0 ? c->tuning.color_levels : kCLevels;
-    t->reserved = 0;
+    t->color_pivots = c->tuning.color_pivots > 0 ? c->tuning.color_pivots : kCPivots;
     return ISPAN_OK;
 }
 

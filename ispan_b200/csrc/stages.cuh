@@ -858,8 +858,9 @@ __global__ void __launch_bounds__(kLocalThreads) k_local_scc(Run<OffT> r, Ext<Of
 // Every active vertex has a priority -- a bijective hash of its id, so
 // priorities are random with respect to the graph -- and a class (initially
 // its WCC).  Each round a sample of the vertices are pivots: those whose
-// priority lies below a threshold that doubles every round (about 1024
-// pivots in the first round, every vertex after log2(n/1024) rounds), plus
+// priority lies below a threshold that doubles every round (about
+// Run::color_pivots -- 1024 by default -- in the first round, every vertex
+// after log2(n/1024) rounds), plus
 // the residual's minimum-priority vertex.  A pivot's colour starts as its
 // priority, every other colour as "none", and colours relax to the minimum
 // over the forward ancestors *inside the class*.  A pivot whose colour is its
@@ -896,6 +897,7 @@ __device__ __forceinline__ uint32_t prio_of(uint32_t v) {
 
 constexpr int kCLQ = 2048;
 constexpr int kCLevels = 32;  // default of Run::color_levels: local levels a CTA works per grid round
+constexpr int kCPivots = 1024;  // default of Run::color_pivots: pivots of the first colouring round
 struct ColorSmem {
     int32_t lq[2][kCLQ];
     int cnt[2];
@@ -1055,7 +1057,7 @@ __global__ void __launch_bounds__(kBlock, 1) k_color(Run<OffT> r, Ext<OffT> x) {
     int shift0 = 0;  // first round: pivots are the priorities below 2^(32 - shift0)
     {   // initial classes: the WCCs (parent holds the WCC root until colours overwrite it)
         const int64_t n = (int64_t)__ldcg(x.ctl + K_LARGE);
-        while (shift0 < 31 && (n >> (shift0 + 1)) >= 1024) ++shift0;
+        while (shift0 < 31 && (n >> (shift0 + 1)) >= r.color_pivots) ++shift0;
         if (blockIdx.x == 0 && threadIdx.x == 0) x.ctl[K_MINPRIO0] = ~0ull;
         if (!grid_sync(r.gsync, r.err)) return;
         uint32_t pm = 0xffffffffu;

@@ -116,8 +116,9 @@ def test_reference_codes_report(ctx):
     assert np.array_equal(oracle.canon_codes(csr, codes), oracle.tarjan(csr))
 
 
-@pytest.mark.parametrize("tun", [dict(async_v=1, async_e=1, async_deg=1, bfs_ctas_per_sm=1, color_levels=1),
-                                 dict(async_v=1 << 22, async_e=1 << 24, async_deg=1024, color_levels=100000),
+@pytest.mark.parametrize("tun", [dict(async_v=1, async_e=1, async_deg=1, bfs_ctas_per_sm=1, color_levels=1, color_pivots=1),
+                                 dict(async_v=1 << 22, async_e=1 << 24, async_deg=1024, color_levels=100000,
+                                      color_pivots=1 << 30),
                                  dict(async_v=4096, async_e=16384, async_deg=4)])
 def test_tuning_does_not_change_labels(tun):
     """The autotuner's launch parameters move time between stages only."""
