@@ -4,16 +4,16 @@ Tuned: the push/pull switch of the reachability searches (alpha, beta, gamma:
 the reference's own knobs, src/fw_bw.h:576-624, whose defaults 30/200/10 come
 from src/bash_one.sh:4), the frontier sizes and vertex degree below which a
 search runs asynchronously inside CTAs (async_v, async_e, async_deg), and
-the CTAs per SM of the persistent searches (bfs_ctas_per_sm), and the local
+the CTAs per SM of the persistent searches (bfs_ctas_per_sm), the local
 levels a CTA works per grid round when colouring large WCCs (color_levels:
-fewer levels balance the CTAs, more save grid barriers) and the pivots of its
-first round (color_pivots).  None of them
-changes a label; they only move time between stages.
+fewer levels balance the CTAs, more save grid barriers) and the pivots of the
+colouring's first round (color_pivots).  None of them changes a label; they
+only move time between stages.
 
 Method: coordinate descent from the defaults over a small grid per
 parameter, two passes, each candidate timed as the median of several runs on
-the device (CUDA events inside the captured graph) of the stages the
-tunables act on (trim and elephant).
+the device (CUDA events inside the captured graph) of the trim, elephant and
+mice stages.
 The winners are stored per shape class in ``tuning_table.json`` beside this
 file; :func:`apply` looks a graph's class up and sets the context.
 
