@@ -880,6 +880,10 @@ __global__ void __launch_bounds__(kLocalThreads) k_local_scc(Run<OffT> r, Ext<Of
 // the drops per vertex near ln(#pivot ancestors) while classes are large and
 // reaches full colouring only once classes are small.
 //
+// A vertex's class and colour share one 64-bit word (class in the high
+// half): an edge check is one load, and a relaxation is one 64-bit atomicMin
+// that cannot change the class (both words have the same high half).
+//
 // Both searches run as asynchronous rounds: each CTA takes a slice of the
 // global frontier and works it to exhaustion with a frontier in shared
 // memory (levels separated by __syncthreads), overflowing to the global
@@ -914,8 +918,7 @@ template <typename OffT, int KIND>
 __device__ __forceinline__ void color_async_round(const Run<OffT> &r, const Ext<OffT> &x, const int32_t *q_in,
                                                   int64_t n_in, int32_t *q_out, unsigned long long *n_out,
                                                   ColorSmem &sm) {
-    uint32_t *col = reinterpret_cast<uint32_t *>(r.parent);
-    const uint32_t *cls = reinterpret_cast<const uint32_t *>(r.qe[0]);
+    unsigned long long *cc = reinterpret_cast<unsigned long long *>(r.qe[0]);  // class << 32 | colour
     int32_t *rootof = r.aux2;
     const OffT *beg = KIND == 0 ? r.fw_beg : r.bw_beg;
     const int32_t *adj = KIND == 0 ? r.fw_adj : r.bw_adj;
@@ -946,27 +949,34 @@ __device__ __forceinline__ void color_async_round(const Run<OffT> &r, const Ext<
                     clear_bit(r.D, v);
                     __threadfence();  // clear the queued mark before reading the colour
                 }
-                cv = __ldcg(col + v);
-                const uint32_t kv = __ldcg(cls + v);
+                // a colour read here may be lowered meanwhile; pushing the
+                // older, larger one is harmless (the lowering re-queues v)
+                const unsigned long long pv = __ldcg(cc + v);
+                cv = (uint32_t)pv;
                 const int32_t rt = KIND == 1 ? __ldcg(rootof + v) : 0;
                 const int64_t e0 = ld_off(beg, v), e1 = ld_off(beg, v + 1);
                 for (int64_t e = e0; e < e1; e += 4) {
                     int32_t w[4];
 #pragma unroll
                     for (int q = 0; q < 4; ++q) w[q] = e + q < e1 ? ld_adj(adj, e + q) : -1;
+                    // one 8-byte load per neighbour carries its class and colour
+                    unsigned long long pw[4];
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) pw[q] = (w[q] >= 0 && w[q] != v) ? __ldcg(cc + w[q]) : 0ull;
                     bool ok[4];
 #pragma unroll
                     for (int q = 0; q < 4; ++q) {
-                        ok[q] = w[q] >= 0 && w[q] != v && bitv(r.A, w[q]);
-                        if (ok[q]) ok[q] = __ldcg(cls + w[q]) == kv;
-                        if (ok[q]) ok[q] = KIND == 0 ? cv < __ldcg(col + w[q])
-                                                     : (__ldcg(col + w[q]) == cv && !bitv(r.F, w[q]));
+                        ok[q] = w[q] >= 0 && w[q] != v && (pw[q] >> 32) == (pv >> 32);
+                        if (ok[q]) ok[q] = KIND == 0 ? cv < (uint32_t)pw[q] : (pw[q] == pv && !bitv(r.F, w[q]));
+                        // inactive vertices keep stale words: the active bit decides
+                        if (ok[q]) ok[q] = bitv(r.A, w[q]);
                     }
 #pragma unroll
                     for (int q = 0; q < 4; ++q) {
                         if (!ok[q]) continue;
                         if (KIND == 0) {
-                            if (cv >= atomicMin(col + w[q], cv)) continue;
+                            // same class in both words: the 64-bit minimum is the colour's
+                            if (cv >= (uint32_t)atomicMin(cc + w[q], pv)) continue;
                             __threadfence();  // the new colour is visible before the mark test
                             if (!set_bit(r.D, w[q])) continue;  // already queued
                         } else {
@@ -1047,8 +1057,9 @@ __global__ void __launch_bounds__(kBlock, 1) k_color(Run<OffT> r, Ext<OffT> x) {
     __shared__ ColorSmem sm;
     const int64_t gt = (int64_t)blockIdx.x * kBlock + threadIdx.x;
     const int64_t nt = (int64_t)gridDim.x * kBlock;
-    uint32_t *col = reinterpret_cast<uint32_t *>(r.parent);
-    uint32_t *cls = reinterpret_cast<uint32_t *>(r.qe[0]);  // class of each vertex
+    // class (high half) and colour (low half) of each vertex in one word
+    unsigned long long *cc = reinterpret_cast<unsigned long long *>(r.qe[0]);
+    const unsigned long long kHi = 0xffffffff00000000ull;
     int32_t *rootof = r.aux2;  // root of the SCC a marked vertex belongs to
     int32_t *mn = r.aux;       // at roots: minimum member id, then the member count
     unsigned long long *cqc = x.ctl + K_CQ0;
@@ -1063,7 +1074,7 @@ __global__ void __launch_bounds__(kBlock, 1) k_color(Run<OffT> r, Ext<OffT> x) {
         uint32_t pm = 0xffffffffu;
         for (int64_t i = gt; i < n; i += nt) {
             int32_t v = x.large[0][i];
-            cls[v] = (uint32_t)r.parent[v];
+            cc[v] = ((unsigned long long)(uint32_t)r.parent[v] << 32) | 0xffffffffull;
             pm = min(pm, prio_of((uint32_t)v));
         }
         pm = __reduce_min_sync(0xffffffffu, pm);
@@ -1098,7 +1109,7 @@ __global__ void __launch_bounds__(kBlock, 1) k_color(Run<OffT> r, Ext<OffT> x) {
                 v = L[i];
                 const uint32_t p = prio_of((uint32_t)v);
                 piv = p < thr || p <= minp;
-                col[v] = piv ? p : 0xffffffffu;
+                cc[v] = (__ldcg(cc + v) & kHi) | (piv ? p : 0xffffffffu);
                 clear_bit(r.F, v);  // F: SCC mark of this round
                 if (piv) set_bit(r.D, v); else clear_bit(r.D, v);  // D: queued mark
             }
@@ -1120,7 +1131,7 @@ __global__ void __launch_bounds__(kBlock, 1) k_color(Run<OffT> r, Ext<OffT> x) {
                 const uint32_t p = prio_of((uint32_t)v);
                 // colours are pivot priorities, so a match means v is a pivot
                 // unless v's priority is the "none" value itself
-                rt = __ldcg(col + v) == p && (p < thr || p <= minp);
+                rt = (uint32_t)__ldcg(cc + v) == p && (p < thr || p <= minp);
                 if (rt) {
                     set_bit(r.F, v);
                     rootof[v] = v;
@@ -1159,8 +1170,10 @@ __global__ void __launch_bounds__(kBlock, 1) k_color(Run<OffT> r, Ext<OffT> x) {
                     ++nl;
                 } else {
                     keep = true;
-                    const uint32_t c = __ldcg(col + v);
-                    if (c != 0xffffffffu) cls[v] = c;  // reached: its colour is its next class
+                    const unsigned long long pv = __ldcg(cc + v);
+                    const uint32_t c = (uint32_t)pv;
+                    // reached: its colour is its next class; unreached: it keeps its class
+                    cc[v] = (c != 0xffffffffu ? ((unsigned long long)c << 32) : (pv & kHi)) | 0xffffffffull;
                     pm = min(pm, prio_of((uint32_t)v));
                 }
             }
