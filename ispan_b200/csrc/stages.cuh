@@ -1052,7 +1052,7 @@ __device__ __forceinline__ int color_async(const Run<OffT> &r, const Ext<OffT> &
 }
 
 template <typename OffT>
-__global__ void __launch_bounds__(kBlock, 1) k_color(Run<OffT> r, Ext<OffT> x) {
+__global__ void __launch_bounds__(kBlock, 2) k_color(Run<OffT> r, Ext<OffT> x) {
     __shared__ int64_t sh[kWarps];
     __shared__ ColorSmem sm;
     const int64_t gt = (int64_t)blockIdx.x * kBlock + threadIdx.x;
