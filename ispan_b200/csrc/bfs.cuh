@@ -259,13 +259,20 @@ __device__ __forceinline__ bool bu_pull(const BfsDir<OffT, DIR> &d, int64_t v, i
 // coalesced load per map) and records the snapshot; the candidates of those
 // words are then dealt out one per lane (n-th set bit selection), so dense
 // and sparse levels both keep every lane busy.  Found bits are combined per
-// word before the atomic OR.
+// word before the atomic OR.  Warps take their 32-word groups from a level
+// counter, so a warp held up by long reverse lists takes fewer groups
+// instead of holding back the grid barrier.
 template <typename OffT, int DIR>
-__device__ __forceinline__ void bu_words(const Run<OffT> &r, const BfsDir<OffT, DIR> &d, int64_t w_begin,
-                                         int64_t w_stride, int64_t &nvis, int64_t &msum_next,
+__device__ __forceinline__ void bu_words(const Run<OffT> &r, const BfsDir<OffT, DIR> &d,
+                                         unsigned long long *next_group, int64_t &nvis, int64_t &msum_next,
                                          int64_t &msum_other) {
     const int lane = lane_id();
-    for (int64_t wb = w_begin * 32; wb < r.W; wb += w_stride * 32) {
+    for (;;) {
+        unsigned long long g = 0;
+        if (lane == 0) g = atomicAdd(next_group, 1ull);
+        g = __shfl_sync(kFull, g, 0);
+        const int64_t wb = (int64_t)g * 32;
+        if (wb >= r.W) break;
         const int64_t my = wb + lane;
         uint32_t vis = my < r.W ? __ldcg(d.Vm + my) : 0u;
         uint32_t cnd = my < r.W ? (__ldg(d.R + my) & ~vis) : 0u;
@@ -478,7 +485,9 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Run<OffT> r, BfsCtl *ctl) {
                 td_chunk<OffT, DIR>(r, d, c, nchunks, qcount, qedges, cur, r.qpk + s_nx, nvis, mnext, mother,
                                     tid, tdsm);
         } else if (mode == M_BU) {
-            bu_words<OffT, DIR>(r, d, gwarp, nwarps, nvis, mnext, mother);
+            // the slot read at this level's start is free until it is
+            // recycled two levels on: its spare word counts the BU groups
+            bu_words<OffT, DIR>(r, d, &slots[s_cur].spare, nvis, mnext, mother);
         } else {
             async_round<OffT, DIR>(r, d, cur, qcount, r.qpk + s_nx, nvis, mnext, mother, asm_);
         }
