@@ -263,15 +263,14 @@ __device__ __forceinline__ bool bu_pull(const BfsDir<OffT, DIR> &d, int64_t v, i
 // counter, so a warp held up by long reverse lists takes fewer groups
 // instead of holding back the grid barrier.
 template <typename OffT, int DIR>
-__device__ __forceinline__ void bu_words(const Run<OffT> &r, const BfsDir<OffT, DIR> &d,
-                                         unsigned long long *next_group, int64_t &nvis, int64_t &msum_next,
-                                         int64_t &msum_other) {
+__device__ __forceinline__ void bu_words(const Run<OffT> &r, const BfsDir<OffT, DIR> &d, int64_t gwarp,
+                                         int64_t nwarps, unsigned long long *next_group, int64_t &nvis,
+                                         int64_t &msum_next, int64_t &msum_other) {
     const int lane = lane_id();
-    for (;;) {
-        unsigned long long g = 0;
-        if (lane == 0) g = atomicAdd(next_group, 1ull);
-        g = __shfl_sync(kFull, g, 0);
-        const int64_t wb = (int64_t)g * 32;
+    // the first group is the warp's own index (no atomic; on small graphs
+    // most warps have none), later ones come from the counter
+    for (int64_t g = gwarp;;) {
+        const int64_t wb = g * 32;
         if (wb >= r.W) break;
         const int64_t my = wb + lane;
         uint32_t vis = my < r.W ? __ldcg(d.Vm + my) : 0u;
@@ -310,6 +309,9 @@ __device__ __forceinline__ void bu_words(const Run<OffT> &r, const BfsDir<OffT, 
                 msum_other += pdeg;
             }
         }
+        unsigned long long nx = 0;
+        if (lane == 0) nx = atomicAdd(next_group, 1ull);
+        g = nwarps + (int64_t)__shfl_sync(kFull, nx, 0);
     }
     (void)msum_next;
 }
@@ -487,7 +489,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Run<OffT> r, BfsCtl *ctl) {
         } else if (mode == M_BU) {
             // the slot read at this level's start is free until it is
             // recycled two levels on: its spare word counts the BU groups
-            bu_words<OffT, DIR>(r, d, &slots[s_cur].spare, nvis, mnext, mother);
+            bu_words<OffT, DIR>(r, d, gwarp, nwarps, &slots[s_cur].spare, nvis, mnext, mother);
         } else {
             async_round<OffT, DIR>(r, d, cur, qcount, r.qpk + s_nx, nvis, mnext, mother, asm_);
         }
