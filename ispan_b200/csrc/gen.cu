@@ -183,9 +183,17 @@ __device__ __forceinline__ int64_t planted_group(int64_t r, int64_t n_core, int6
 
 __global__ void k_planted_min(Perm perm, int64_t n, int64_t n_core, int64_t block_lo, const int64_t *bnd,
                               int64_t nb, int32_t *gmin) {
-    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t gi = planted_group(r, n_core, block_lo, bnd, nb);
-        if (gi >= 0) atomicMin(gmin + gi, (int32_t)perm.vertex(r));
+    // grid-stride with whole warps in every iteration, so lanes of the same
+    // group (the core is a third of all ranks) combine before one atomic
+    const int lane = threadIdx.x & 31;
+    for (int64_t r0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x - lane; r0 < n;
+         r0 += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t r = r0 + lane;
+        const int64_t gi = r < n ? planted_group(r, n_core, block_lo, bnd, nb) : -1;
+        const uint32_t v = r < n ? (uint32_t)perm.vertex(r) : 0xffffffffu;
+        const unsigned grp = __match_any_sync(0xffffffffu, (unsigned long long)gi);
+        const uint32_t mv = __reduce_min_sync(grp, v);
+        if (gi >= 0 && lane == __ffs(grp) - 1) atomicMin(gmin + gi, (int32_t)mv);
     }
 }
 
