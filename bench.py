@@ -583,10 +583,12 @@ def main():
     ws, rank, local = dist_init()
     import torch
 
-    if args.workload == "batch" and args.impl == "ours":
-        return bench_batch(args, ws, rank, local)
-    if args.workload == "served" and args.impl == "ours":
-        return bench_served(args, ws, rank, local)
+    if args.workload in ("batch", "served") and args.impl == "ours":
+        (bench_batch if args.workload == "batch" else bench_served)(args, ws, rank, local)
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
 
     if args.impl == "reference":
         if rank != 0:
