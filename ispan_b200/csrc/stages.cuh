@@ -415,13 +415,22 @@ __device__ __forceinline__ int distinct_active(const OffT *beg, const int32_t *a
                                                int32_t x1, int32_t x2, int cap, int32_t &n1, int32_t &n2) {
     int64_t e0 = ld_off(beg, v), e1 = ld_off(beg, v + 1);
     int d = 0;
-    for (int64_t e = e0; e < e1; ++e) {
-        int32_t w = ld_adj(adj, e);
-        if (w == x1 || w == x2 || !bitv(A, w)) continue;
-        if (d == 0) { n1 = w; d = 1; }
-        else if (d == 1 && w != n1) { n2 = w; d = 2; }
-        else if (d == 2 && w != n1 && w != n2) { d = 3; }
-        if (d >= cap) break;
+    // four edges per step: their ids, then their active bits, each group of
+    // loads in flight together; the early exit stays per edge
+    for (int64_t e = e0; e < e1 && d < cap; e += 4) {
+        int32_t w[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) w[q] = e + q < e1 ? ld_adj(adj, e + q) : -1;
+        bool act[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) act[q] = w[q] >= 0 && w[q] != x1 && w[q] != x2 && bitv(A, w[q]);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            if (!act[q] || d >= cap) continue;
+            if (d == 0) { n1 = w[q]; d = 1; }
+            else if (d == 1 && w[q] != n1) { n2 = w[q]; d = 2; }
+            else if (d == 2 && w[q] != n1 && w[q] != n2) { d = 3; }
+        }
     }
     return d;
 }
