@@ -560,18 +560,27 @@ __global__ void __launch_bounds__(kBlock) k_wcc_hook(Run<OffT> r, Ext<OffT> x, i
     for (int64_t i = (int64_t)blockIdx.x * kBlock + threadIdx.x; i < n; i += (int64_t)gridDim.x * kBlock) {
         int32_t v = r.wl[in][i];
         int64_t e0 = ld_off(r.fw_beg, v), e1 = ld_off(r.fw_beg, v + 1);
-        for (int64_t e = e0; e < e1; ++e) {
-            int32_t w = ld_adj(r.fw_adj, e);
-            if (w == v || !bitc(r.A, w)) continue;
-            int32_t a = v, b = w;
-            for (int guard = 0; guard < (1 << 20); ++guard) {
-                a = uf_find(r.parent, a);
-                b = uf_find(r.parent, b);
-                if (a == b) break;
-                if (a > b) { int32_t t = a; a = b; b = t; }
-                int32_t old = atomicCAS(r.parent + b, b, a);  // hook root b under a
-                if (old == b) break;
-                b = old;
+        for (int64_t e = e0; e < e1; e += 4) {
+            // four neighbours' ids, then their active bits, in flight together
+            int32_t ws[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) ws[q] = e + q < e1 ? ld_adj(r.fw_adj, e + q) : v;
+            bool act[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) act[q] = ws[q] != v && bitc(r.A, ws[q]);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                if (!act[q]) continue;
+                int32_t a = v, b = ws[q];
+                for (int guard = 0; guard < (1 << 20); ++guard) {
+                    a = uf_find(r.parent, a);
+                    b = uf_find(r.parent, b);
+                    if (a == b) break;
+                    if (a > b) { int32_t t = a; a = b; b = t; }
+                    int32_t old = atomicCAS(r.parent + b, b, a);  // hook root b under a
+                    if (old == b) break;
+                    b = old;
+                }
             }
         }
     }
