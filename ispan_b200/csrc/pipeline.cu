@@ -61,8 +61,6 @@ struct ispan_ctx {
     int nsm = 148;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
-    cudaStream_t up_stream = nullptr;  // second copy stream for host uploads
-    cudaEvent_t up_ev[2] = {nullptr, nullptr};
     int64_t maxV = 0, maxE = 0, maxW = 0;
     int64_t maxSeg = 0;
     std::vector<void *> owned;      // fixed scratch
@@ -622,23 +620,12 @@ static int upload(ispan_ctx *c, const ispan_csr *g) {
         c->up_V = g->V;
         c->up_E = g->E;
     }
-    // the forward arrays on the run's stream, the backward ones on a second
-    // stream, so both copy engines work; the run waits for both
-    if (!c->up_stream) {
-        CK(cudaStreamCreateWithFlags(&c->up_stream, cudaStreamNonBlocking));
-        CK(cudaEventCreateWithFlags(&c->up_ev[0], cudaEventDisableTiming));
-        CK(cudaEventCreateWithFlags(&c->up_ev[1], cudaEventDisableTiming));
-    }
-    CK(cudaEventRecord(c->up_ev[0], c->stream));  // earlier work on the buffers is done first
-    CK(cudaStreamWaitEvent(c->up_stream, c->up_ev[0], 0));
     CK(cudaMemcpyAsync(c->up_fw_beg, g->fw_beg, (size_t)(g->V + 1) * ob, cudaMemcpyHostToDevice, c->stream));
-    CK(cudaMemcpyAsync(c->up_bw_beg, g->bw_beg, (size_t)(g->V + 1) * ob, cudaMemcpyHostToDevice, c->up_stream));
+    CK(cudaMemcpyAsync(c->up_bw_beg, g->bw_beg, (size_t)(g->V + 1) * ob, cudaMemcpyHostToDevice, c->stream));
     if (g->E) {
         CK(cudaMemcpyAsync(c->up_fw_adj, g->fw_adj, (size_t)g->E * 4, cudaMemcpyHostToDevice, c->stream));
-        CK(cudaMemcpyAsync(c->up_bw_adj, g->bw_adj, (size_t)g->E * 4, cudaMemcpyHostToDevice, c->up_stream));
+        CK(cudaMemcpyAsync(c->up_bw_adj, g->bw_adj, (size_t)g->E * 4, cudaMemcpyHostToDevice, c->stream));
     }
-    CK(cudaEventRecord(c->up_ev[1], c->up_stream));
-    CK(cudaStreamWaitEvent(c->stream, c->up_ev[1], 0));
     return ISPAN_OK;
 }
 
@@ -931,12 +918,6 @@ int ispan_ctx_destroy(ispan_ctx *c) {
         for (int i = 0; i < 12; ++i) cudaEventDestroy(c->ev[i]);
     if (c->h_counters) cudaFreeHost(c->h_counters);
     if (c->h_err) cudaFreeHost(c->h_err);
-    if (c->up_stream) {
-        cudaStreamSynchronize(c->up_stream);
-        cudaStreamDestroy(c->up_stream);
-    }
-    for (cudaEvent_t e : c->up_ev)
-        if (e) cudaEventDestroy(e);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return ISPAN_OK;
