@@ -254,6 +254,13 @@ int ispan_ref_codes(ispan_ctx *ctx, int32_t *codes_out);
  * print the same kind of record). */
 int ispan_debug_trace(ispan_ctx *ctx, int64_t *out, int64_t cap);
 
+/* Failure detection, exercised without a GPU fault: runs the persistent
+ * stages' bounded grid barrier with a CTA that never arrives and a limit of
+ * limit_us (at most 10 s); the waiting CTA gives up, records
+ * ISPAN_ERR_TIMEOUT and returns, which this call returns.  The context stays
+ * usable.  No counterpart in the reference (it has no bounded waits). */
+int ispan_debug_barrier_timeout(ispan_ctx *ctx, int64_t limit_us);
+
 const char *ispan_strerror(int code);
 /* library version string */
 const char *ispan_version(void);

@@ -258,7 +258,7 @@ __device__ __forceinline__ unsigned atom_add_acqrel_u32(unsigned *p, unsigned v)
     return old;
 }
 
-__device__ __noinline__ bool grid_sync(unsigned *gs, int *err) {
+__device__ __noinline__ bool grid_sync(unsigned *gs, int *err, uint64_t limit_ns = kBarrierTimeoutNs) {
     __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -277,7 +277,7 @@ __device__ __noinline__ bool grid_sync(unsigned *gs, int *err) {
             while (ld_acquire_u32(gs + 1) == gen) {
                 if ((++spin & 63) == 0) {
                     if (ld_volatile_int(err) != 0) { ok = 0; break; }
-                    if (globaltimer() - t0 > kBarrierTimeoutNs) {
+                    if (globaltimer() - t0 > limit_ns) {
                         atomicCAS(err, 0, kErrTimeout);
                         ok = 0;
                         break;

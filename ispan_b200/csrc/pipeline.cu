@@ -54,6 +54,15 @@ static int dalloc(T **p, size_t n, std::vector<void *> &owned) {
     return ISPAN_OK;
 }
 
+// Failure-detection probe: a two-CTA grid whose second CTA never reaches
+// the barrier, so the first waits in grid_sync until its time limit, sets
+// the error word and returns (the same bounded wait every persistent stage
+// uses, with a short limit).
+__global__ void k_barrier_probe(unsigned *gs, int *err, uint64_t limit_ns) {
+    if (blockIdx.x == 1) return;  // this CTA never arrives
+    grid_sync(gs, err, limit_ns);
+}
+
 }  // namespace
 
 struct ispan_ctx {
@@ -1024,6 +1033,24 @@ int ispan_ref_codes(ispan_ctx *c, int32_t *codes) {
     }
     codes[V] = 0;
     return ISPAN_OK;
+}
+
+int ispan_debug_barrier_timeout(ispan_ctx *c, int64_t limit_us) {
+    if (!c || limit_us <= 0 || limit_us > 10 * 1000 * 1000) return ISPAN_ERR_ARG;
+    std::lock_guard<std::mutex> lock(c->mu);
+    if (cudaSetDevice(c->device) != cudaSuccess) return ISPAN_ERR_CUDA;
+    CK(cudaMemsetAsync(c->gsync, 0, 4 * sizeof(unsigned), c->stream));
+    CK(cudaMemsetAsync(c->err, 0, 4 * sizeof(int), c->stream));
+    k_barrier_probe<<<2, 32, 0, c->stream>>>(c->gsync, c->err, (uint64_t)limit_us * 1000ull);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(c->h_err, c->err, 4 * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    const int e = c->h_err[0];
+    // leave the barrier state clean for the next run (runs reset it too)
+    CK(cudaMemsetAsync(c->gsync, 0, 4 * sizeof(unsigned), c->stream));
+    CK(cudaMemsetAsync(c->err, 0, 4 * sizeof(int), c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return e;
 }
 
 int ispan_debug_trace(ispan_ctx *c, int64_t *out, int64_t cap) {
