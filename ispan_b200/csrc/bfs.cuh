@@ -267,15 +267,20 @@ __device__ __forceinline__ void bu_words(const Run<OffT> &r, const BfsDir<OffT, 
                                          int64_t nwarps, unsigned long long *next_group, int64_t &nvis,
                                          int64_t &msum_next, int64_t &msum_other) {
     const int lane = lane_id();
+    // words per group: 32 (one per lane) when there are groups enough for
+    // every warp, fewer on small graphs so that more warps get candidates
+    int gsz = 32;
+    while (gsz > 1 && (int64_t)(r.W + gsz - 1) / gsz < nwarps) gsz >>= 1;
     // the first group is the warp's own index (no atomic; on small graphs
     // most warps have none), later ones come from the counter
     for (int64_t g = gwarp;;) {
-        const int64_t wb = g * 32;
+        const int64_t wb = g * gsz;
         if (wb >= r.W) break;
         const int64_t my = wb + lane;
-        uint32_t vis = my < r.W ? __ldcg(d.Vm + my) : 0u;
-        uint32_t cnd = my < r.W ? (__ldg(d.R + my) & ~vis) : 0u;
-        if (my < r.W) r.P[my] = vis;  // snapshot for a later switch to top-down
+        const bool mine = lane < gsz && my < r.W;
+        uint32_t vis = mine ? __ldcg(d.Vm + my) : 0u;
+        uint32_t cnd = mine ? (__ldg(d.R + my) & ~vis) : 0u;
+        if (mine) r.P[my] = vis;  // snapshot for a later switch to top-down
         int c = __popc(cnd), incl = c;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
