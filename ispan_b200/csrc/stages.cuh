@@ -1079,7 +1079,8 @@ __global__ void __launch_bounds__(kBlock, 2) k_color(Run<OffT> r, Ext<OffT> x) {
     unsigned long long *cc = reinterpret_cast<unsigned long long *>(r.qe[0]);
     const unsigned long long kHi = 0xffffffff00000000ull;
     int32_t *rootof = r.aux2;  // root of the SCC a marked vertex belongs to
-    int32_t *mn = r.aux;       // at roots: minimum member id, then the member count
+    int32_t *mn = r.aux;       // at roots: minimum member id
+    int32_t *szc = r.cnt_in;   // at roots: member count (the peel's counters are done)
     unsigned long long *cqc = x.ctl + K_CQ0;
     int cur = 0, rounds = 0;
     int64_t prev_n = INT64_MAX;
@@ -1154,6 +1155,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_color(Run<OffT> r, Ext<OffT> x) {
                     set_bit(r.F, v);
                     rootof[v] = v;
                     mn[v] = v;
+                    szc[v] = 0;
                 }
             }
             wl_append(rt, v, x.cq[0], cqc + 0);
@@ -1170,22 +1172,38 @@ __global__ void __launch_bounds__(kBlock, 2) k_color(Run<OffT> r, Ext<OffT> x) {
             t[2] = npiv;
             t[3] = (long long)globaltimer();
         }
-        for (int64_t i = gt; i < n; i += nt) {  // minimum member id per SCC
+        for (int64_t i = gt; i < n; i += nt) {  // minimum member id and size per SCC
             int32_t v = L[i];
-            if (bitv(r.F, v)) atomicMin(mn + __ldcg(rootof + v), v);
+            if (bitv(r.F, v)) {
+                const int32_t rv = __ldcg(rootof + v);
+                atomicMin(mn + rv, v);
+                atomicAdd(szc + rv, 1);
+            }
         }
         if (!grid_sync(r.gsync, r.err)) return;
-        int64_t nl = 0;
+        int64_t nl = 0, nroots = 0;
         uint32_t pm = 0xffffffffu;
-        for (int64_t i = gt; i - threadIdx.x < n; i += nt) {  // labels; the rest continues
+        for (int64_t i = gt; i - threadIdx.x < n; i += nt) {  // labels, sizes; the rest continues
             bool keep = false;
             int32_t v = 0;
             if (i < n) {
                 v = L[i];
                 if (bitv(r.F, v)) {
-                    r.label[v] = __ldcg(mn + __ldcg(rootof + v));
+                    const int32_t rv = __ldcg(rootof + v);
+                    r.label[v] = __ldcg(mn + rv);
                     r.cls[v] = CLS_MICE;
+                    clear_bit(r.A, v);
                     ++nl;
+                    if (rv == v) {  // one histogram entry per SCC, at its root
+                        const int32_t sz = __ldcg(szc + v);
+                        if (sz < kHistCap) {
+                            atomicAdd((unsigned long long *)(r.hist + sz), 1ull);
+                        } else {
+                            unsigned long long k = atomicAdd(r.counters + C_BIG, 1ull);
+                            if (k < kBigCap) r.hist[kHistCap + k] = sz;
+                        }
+                        ++nroots;
+                    }
                 } else {
                     keep = true;
                     const unsigned long long pv = __ldcg(cc + v);
@@ -1199,34 +1217,6 @@ __global__ void __launch_bounds__(kBlock, 2) k_color(Run<OffT> r, Ext<OffT> x) {
         }
         pm = __reduce_min_sync(0xffffffffu, pm);
         if ((threadIdx.x & 31) == 0 && pm != 0xffffffffu) atomicMin(next_minp, (unsigned long long)pm);
-        if (!grid_sync(r.gsync, r.err)) return;
-        for (int64_t i = gt; i < n; i += nt) {  // sizes: reuse mn at the roots
-            int32_t v = L[i];
-            if (bitv(r.F, v) && __ldcg(rootof + v) == v) mn[v] = 0;
-        }
-        if (!grid_sync(r.gsync, r.err)) return;
-        for (int64_t i = gt; i < n; i += nt) {
-            int32_t v = L[i];
-            if (bitv(r.F, v)) atomicAdd(mn + __ldcg(rootof + v), 1);
-        }
-        if (!grid_sync(r.gsync, r.err)) return;
-        int64_t nroots = 0;
-        for (int64_t i = gt; i < n; i += nt) {
-            int32_t v = L[i];
-            if (bitv(r.F, v)) {
-                clear_bit(r.A, v);
-                if (__ldcg(rootof + v) == v) {
-                    int32_t sz = __ldcg(mn + v);
-                    if (sz < kHistCap) {
-                        atomicAdd((unsigned long long *)(r.hist + sz), 1ull);
-                    } else {
-                        unsigned long long k = atomicAdd(r.counters + C_BIG, 1ull);
-                        if (k < kBigCap) r.hist[kHistCap + k] = sz;
-                    }
-                    ++nroots;
-                }
-            }
-        }
         int64_t a = block_sum64(nl, sh), b = block_sum64(nroots, sh);
         if (threadIdx.x == 0) {
             if (a) atomicAdd(r.counters + C_MICE_V, (unsigned long long)a);
