@@ -215,6 +215,18 @@ int ispan_server_destroy(ispan_server *s);
 int ispan_condense(const ispan_csr *g, const int32_t *labels, uint64_t *pairs_out, int64_t cap,
                    int64_t *n_pairs, void *stream);
 
+/* One rank's level of a reachability search over a graph whose rows are
+ * split across GPUs: rows holds the CSR rows of the vertices [v0, v0 +
+ * rows->V) (forward rows for a forward search, backward rows for a backward
+ * one; fw_beg/fw_adj are read, offsets local, adjacency global ids, device
+ * memory).  Every owned vertex set in frontier[] (byte per vertex, V
+ * entries) marks next[w] = 1 for each neighbour w not in visited[] and, if
+ * allowed is not NULL, set in allowed[].  The caller merges the ranks' next
+ * maps with a MAX all-reduce (ispan_b200/sharded.py).  Replaces the per-level
+ * step of the reference's MPI variant (src_mpi/fw_bw.h:382-442). */
+int ispan_shard_expand(const ispan_csr *rows, int64_t v0, int64_t V, const uint8_t *frontier,
+                       const uint8_t *visited, const uint8_t *allowed, uint8_t *next, void *stream);
+
 /* Largest graph (vertices) that ispan_scc_small_noalloc accepts. */
 #define ISPAN_NOALLOC_MAX_V 65536
 
