@@ -898,9 +898,15 @@ __global__ void __launch_bounds__(kLocalThreads) k_local_scc(Run<OffT> r, Ext<Of
 // the drops per vertex near ln(#pivot ancestors) while classes are large and
 // reaches full colouring only once classes are small.
 //
-// A vertex's class and colour share one 64-bit word (class in the high
-// half): an edge check is one load, and a relaxation is one 64-bit atomicMin
-// that cannot change the class (both words have the same high half).
+// A vertex's class, colour and queued flag share one 64-bit word: class in
+// the high half, the 31-bit colour in bits 31..1, and bit 0 set while the
+// vertex is NOT in a queue.  An edge check is one load; a relaxation is one
+// compare-and-swap that lowers the colour and clears the flag, so the thread
+// whose relaxation found the flag set is the one that queues the vertex; a
+// pop is one atomicOr that sets the flag and returns the current colour.
+// Vertices outside the large WCCs carry the class 0xffffffff, which no live
+// class equals (classes are WCC roots and colours, both below 2^31 - 1), so
+// the class compare also rejects inactive neighbours.
 //
 // Both searches run as asynchronous rounds: each CTA takes a slice of the
 // global frontier and works it to exhaustion with a frontier in shared
@@ -908,14 +914,19 @@ __global__ void __launch_bounds__(kLocalThreads) k_local_scc(Run<OffT> r, Ext<Of
 // queue; a grid barrier separates rounds, so ring-shaped SCCs cost no grid
 // barrier per hop.
 __device__ __forceinline__ uint32_t prio_of(uint32_t v) {
-    // bijection on 32 bits: xor-shifts and odd multipliers are invertible
+    // bijection on [0, 2^31): xor-shifts and odd multipliers mod 2^31 are
+    // invertible there
+    v &= 0x7fffffffu;
     v ^= v >> 16;
-    v *= 0x7feb352du;
+    v = (v * 0x7feb352du) & 0x7fffffffu;
     v ^= v >> 15;
-    v *= 0x846ca68bu;
+    v = (v * 0x846ca68bu) & 0x7fffffffu;
     v ^= v >> 16;
     return v;
 }
+constexpr uint32_t kNoColour = 0x7fffffffu;            // "no pivot reached this vertex"
+constexpr unsigned long long kDeadWord = ~0ull;        // class 0xffffffff: outside the large WCCs
+__device__ __forceinline__ uint32_t colour_of(unsigned long long w) { return ((uint32_t)w) >> 1; }
 
 constexpr int kCLQ = 2048;
 constexpr int kCLevels = 32;  // default of Run::color_levels: local levels a CTA works per grid round
@@ -962,15 +973,12 @@ __device__ __forceinline__ void color_async_round(const Run<OffT> &r, const Ext<
             if (n == 0) break;  // the slice is consumed too (the refill keeps the frontier non-empty)
             for (int i = tid; i < n; i += kBlock) {
                 const int32_t v = sm.lq[c][i];
-                uint32_t cv;
-                if (KIND == 0) {
-                    clear_bit(r.D, v);
-                    __threadfence();  // clear the queued mark before reading the colour
-                }
-                // a colour read here may be lowered meanwhile; pushing the
-                // older, larger one is harmless (the lowering re-queues v)
-                const unsigned long long pv = __ldcg(cc + v);
-                cv = (uint32_t)pv;
+                // KIND 0: leaving the queue sets the flag and reads the colour in
+                // one atomic; a lowering after it queues v again.  A colour read
+                // here may be lowered meanwhile; pushing the older, larger one is
+                // harmless (that lowering re-queues v).
+                const unsigned long long pv = KIND == 0 ? atomicOr(cc + v, 1ull) : __ldcg(cc + v);
+                const uint32_t cv = colour_of(pv);
                 const int32_t rt = KIND == 1 ? __ldcg(rootof + v) : 0;
                 const int64_t e0 = ld_off(beg, v), e1 = ld_off(beg, v + 1);
                 for (int64_t e = e0; e < e1; e += 4) {
@@ -984,19 +992,31 @@ __device__ __forceinline__ void color_async_round(const Run<OffT> &r, const Ext<
                     bool ok[4];
 #pragma unroll
                     for (int q = 0; q < 4; ++q) {
+                        // the class compare also rejects inactive neighbours (dead class)
                         ok[q] = w[q] >= 0 && w[q] != v && (pw[q] >> 32) == (pv >> 32);
-                        if (ok[q]) ok[q] = KIND == 0 ? cv < (uint32_t)pw[q] : (pw[q] == pv && !bitv(r.F, w[q]));
-                        // inactive vertices keep stale words: the active bit decides
-                        if (ok[q]) ok[q] = bitv(r.A, w[q]);
+                        if (ok[q])
+                            ok[q] = KIND == 0 ? cv < colour_of(pw[q])
+                                              : (((pw[q] ^ pv) >> 1) == 0 && !bitv(r.F, w[q]));
                     }
 #pragma unroll
                     for (int q = 0; q < 4; ++q) {
                         if (!ok[q]) continue;
                         if (KIND == 0) {
-                            // same class in both words: the 64-bit minimum is the colour's
-                            if (cv >= (uint32_t)atomicMin(cc + w[q], pv)) continue;
-                            __threadfence();  // the new colour is visible before the mark test
-                            if (!set_bit(r.D, w[q])) continue;  // already queued
+                            // lower the colour and clear the flag; the class cannot
+                            // change under a successful swap (it is compared first)
+                            const unsigned long long nw = (pv & 0xffffffff00000000ull) | ((unsigned long long)cv << 1);
+                            unsigned long long old = pw[q];
+                            bool lowered = false;
+                            int t = 0;
+                            // every failed swap saw a lower colour or a pop's flag
+                            for (; t < (1 << 20); ++t) {
+                                if ((old >> 32) != (pv >> 32) || colour_of(old) <= cv) break;
+                                const unsigned long long seen = atomicCAS(cc + w[q], old, nw);
+                                if (seen == old) { lowered = true; break; }
+                                old = seen;
+                            }
+                            if (t == (1 << 20)) atomicCAS(r.err, 0, kErrOverflow);
+                            if (!lowered || !(old & 1ull)) continue;  // not lowered, or already queued
                         } else {
                             if (!set_bit(r.F, w[q])) continue;
                             rootof[w[q]] = rt;
@@ -1087,13 +1107,16 @@ __global__ void __launch_bounds__(kBlock, 2) k_color(Run<OffT> r, Ext<OffT> x) {
     int shift0 = 0;  // first round: pivots are the priorities below 2^(32 - shift0)
     {   // initial classes: the WCCs (parent holds the WCC root until colours overwrite it)
         const int64_t n = (int64_t)__ldcg(x.ctl + K_LARGE);
-        while (shift0 < 31 && (n >> (shift0 + 1)) >= r.color_pivots) ++shift0;
+        while (shift0 < 30 && (n >> (shift0 + 1)) >= r.color_pivots) ++shift0;
         if (blockIdx.x == 0 && threadIdx.x == 0) x.ctl[K_MINPRIO0] = ~0ull;
+        if (n == 0) return;
+        // every word dead first: neighbours outside the large WCCs fail the class compare
+        for (int64_t i = gt; i < r.V; i += nt) cc[i] = kDeadWord;
         if (!grid_sync(r.gsync, r.err)) return;
         uint32_t pm = 0xffffffffu;
         for (int64_t i = gt; i < n; i += nt) {
             int32_t v = x.large[0][i];
-            cc[v] = ((unsigned long long)(uint32_t)r.parent[v] << 32) | 0xffffffffull;
+            cc[v] = ((unsigned long long)(uint32_t)r.parent[v] << 32) | ((unsigned long long)kNoColour << 1) | 1ull;
             pm = min(pm, prio_of((uint32_t)v));
         }
         pm = __reduce_min_sync(0xffffffffu, pm);
@@ -1112,7 +1135,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_color(Run<OffT> r, Ext<OffT> x) {
         const int32_t *L = x.large[cur];
         // pivots: priority below the round's threshold, or the residual's minimum
         const int shift = max(0, shift0 - (rounds - 1));
-        const unsigned long long thr = 1ull << (32 - shift);
+        const unsigned long long thr = 1ull << (31 - shift);
         const unsigned long long minp = __ldcg(x.ctl + K_MINPRIO0 + cur);
         unsigned long long *next_minp = x.ctl + K_MINPRIO0 + (cur ^ 1);
         if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -1128,9 +1151,9 @@ __global__ void __launch_bounds__(kBlock, 2) k_color(Run<OffT> r, Ext<OffT> x) {
                 v = L[i];
                 const uint32_t p = prio_of((uint32_t)v);
                 piv = p < thr || p <= minp;
-                cc[v] = (__ldcg(cc + v) & kHi) | (piv ? p : 0xffffffffu);
+                // a pivot starts queued (flag clear) with its priority as colour
+                cc[v] = (__ldcg(cc + v) & kHi) | (piv ? (unsigned long long)p << 1 : ((unsigned long long)kNoColour << 1) | 1ull);
                 clear_bit(r.F, v);  // F: SCC mark of this round
-                if (piv) set_bit(r.D, v); else clear_bit(r.D, v);  // D: queued mark
             }
             wl_append(piv, v, x.cq[0], cqc + 0);
         }
@@ -1150,7 +1173,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_color(Run<OffT> r, Ext<OffT> x) {
                 const uint32_t p = prio_of((uint32_t)v);
                 // colours are pivot priorities, so a match means v is a pivot
                 // unless v's priority is the "none" value itself
-                rt = (uint32_t)__ldcg(cc + v) == p && (p < thr || p <= minp);
+                rt = colour_of(__ldcg(cc + v)) == p && (p < thr || p <= minp);
                 if (rt) {
                     set_bit(r.F, v);
                     rootof[v] = v;
@@ -1193,6 +1216,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_color(Run<OffT> r, Ext<OffT> x) {
                     r.label[v] = __ldcg(mn + rv);
                     r.cls[v] = CLS_MICE;
                     clear_bit(r.A, v);
+                    cc[v] = kDeadWord;
                     ++nl;
                     if (rv == v) {  // one histogram entry per SCC, at its root
                         const int32_t sz = __ldcg(szc + v);
@@ -1207,9 +1231,10 @@ __global__ void __launch_bounds__(kBlock, 2) k_color(Run<OffT> r, Ext<OffT> x) {
                 } else {
                     keep = true;
                     const unsigned long long pv = __ldcg(cc + v);
-                    const uint32_t c = (uint32_t)pv;
+                    const uint32_t c = colour_of(pv);
                     // reached: its colour is its next class; unreached: it keeps its class
-                    cc[v] = (c != 0xffffffffu ? ((unsigned long long)c << 32) : (pv & kHi)) | 0xffffffffull;
+                    cc[v] = (c != kNoColour ? ((unsigned long long)c << 32) : (pv & kHi)) |
+                            ((unsigned long long)kNoColour << 1) | 1ull;
                     pm = min(pm, prio_of((uint32_t)v));
                 }
             }
