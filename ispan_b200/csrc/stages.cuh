@@ -928,142 +928,166 @@ constexpr uint32_t kNoColour = 0x7fffffffu;            // "no pivot reached this
 constexpr unsigned long long kDeadWord = ~0ull;        // class 0xffffffff: outside the large WCCs
 __device__ __forceinline__ uint32_t colour_of(unsigned long long w) { return ((uint32_t)w) >> 1; }
 
-constexpr int kCLQ = 2048;
-constexpr int kCLevels = 32;  // default of Run::color_levels: local levels a CTA works per grid round
+constexpr int kCWQ = 256;     // per-warp frontier ring (entries); a power of two
+constexpr int kCLevels = 32;  // default of Run::color_levels: a warp works up to 4 * color_levels chunks of 32 entries per grid round
 constexpr int kCPivots = 1024;  // default of Run::color_pivots: pivots of the first colouring round
 struct ColorSmem {
-    int32_t lq[2][kCLQ];
-    int cnt[2];
-    int take;  // slice entries joining the next level
-    int rem;   // handed back: the frontier entries and the unread slice
-    unsigned long long base;
+    int32_t ring[kWarps][kCWQ];
+    unsigned long long cursor;  // next unread entry of this CTA's slice of the grid queue
 };
 
 // One asynchronous round over the global queue q_in[0..n_in).  KIND 0
 // relaxes colours forward inside the class (push the smaller colour to
 // out-neighbours of the same class, re-queueing them); KIND 1 grows each
 // root's SCC backward inside its colour (claim in-neighbours in F).
+//
+// Every warp works on its own: it takes 32 entries at a time from its ring
+// in shared memory, or from the CTA's slice of the grid queue when the ring
+// is empty, spreads the chunk's edges evenly over its lanes (a warp prefix
+// sum over the degrees, each lane finding its edge's owner by a binary
+// search over the prefix), and appends the vertices it queues to its ring
+// (the grid queue when the ring is full).  No barrier between warps: a warp
+// with a long list or slow loads delays no other.  After 4 * color_levels
+// chunks a warp hands its ring back to the grid queue, and the CTA hands
+// back the unread rest of its slice, so no CTA keeps the grid barrier
+// waiting; the next grid round spreads that work over all CTAs.
 template <typename OffT, int KIND>
 __device__ __forceinline__ void color_async_round(const Run<OffT> &r, const Ext<OffT> &x, const int32_t *q_in,
                                                   int64_t n_in, int32_t *q_out, unsigned long long *n_out,
                                                   ColorSmem &sm) {
-    unsigned long long *cc = reinterpret_cast<unsigned long long *>(r.qe[0]);  // class << 32 | colour
+    unsigned long long *cc = reinterpret_cast<unsigned long long *>(r.qe[0]);  // class | colour | flag
     int32_t *rootof = r.aux2;
     const OffT *beg = KIND == 0 ? r.fw_beg : r.bw_beg;
     const int32_t *adj = KIND == 0 ? r.fw_adj : r.bw_adj;
-    const int tid = threadIdx.x;
-    // This CTA's slice of the queue feeds its local frontier as room frees
-    // up, so the searches started from all of the slice's entries advance
-    // together, level by level (working the slice in separate chunks would
-    // pay the depth of a search once per chunk).
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = lanemask_lt();
+    int32_t *ring = sm.ring[threadIdx.x >> 5];
     const int64_t s0 = n_in * blockIdx.x / gridDim.x, s1 = n_in * (blockIdx.x + 1) / gridDim.x;
-    int64_t next_in = s0;
-    {
-        const int n0 = (int)min((int64_t)kCLQ, s1 - s0);
-        __syncthreads();
-        for (int i = tid; i < n0; i += kBlock) sm.lq[0][i] = __ldcg(q_in + s0 + i);
-        if (tid == 0) { sm.cnt[0] = n0; sm.cnt[1] = 0; }
-        next_in += n0;
-        __syncthreads();
-    }
-    {
-        int c = 0;
-        for (int it = 0; it < (1 << 30); ++it) {
-            const int n = sm.cnt[c];
-            if (n == 0) break;  // the slice is consumed too (the refill keeps the frontier non-empty)
-            for (int i = tid; i < n; i += kBlock) {
-                const int32_t v = sm.lq[c][i];
-                // KIND 0: leaving the queue sets the flag and reads the colour in
-                // one atomic; a lowering after it queues v again.  A colour read
-                // here may be lowered meanwhile; pushing the older, larger one is
-                // harmless (that lowering re-queues v).
-                const unsigned long long pv = KIND == 0 ? atomicOr(cc + v, 1ull) : __ldcg(cc + v);
-                const uint32_t cv = colour_of(pv);
-                const int32_t rt = KIND == 1 ? __ldcg(rootof + v) : 0;
-                const int64_t e0 = ld_off(beg, v), e1 = ld_off(beg, v + 1);
-                for (int64_t e = e0; e < e1; e += 4) {
-                    int32_t w[4];
+    __syncthreads();  // the previous round's readers of the cursor are done
+    if (threadIdx.x == 0) sm.cursor = (unsigned long long)s0;
+    __syncthreads();
+    int head = 0, tail = 0;  // ring [head, tail), warp-uniform
+    const int cap = 4 * r.color_levels;
+    bool capped = false;
+    for (int chunk = 0;; ++chunk) {
+        if (chunk >= cap) { capped = true; break; }
+        int nb;
+        int32_t v = -1;
+        if (tail != head) {
+            nb = min(32, tail - head);
+            if (lane < nb) v = ring[(head + lane) & (kCWQ - 1)];
+            head += nb;
+        } else {
+            unsigned long long g = 0;
+            if (lane == 0) g = atomicAdd(&sm.cursor, 32ull);
+            g = __shfl_sync(kFull, g, 0);
+            if ((int64_t)g >= s1) break;
+            nb = (int)min((int64_t)32, s1 - (int64_t)g);
+            if (lane < nb) v = __ldcg(q_in + g + lane);
+        }
+        __syncwarp();  // ring slots read above may be refilled below
+        // the chunk's vertices: KIND 0 leaves the queue here (sets the flag and
+        // reads the colour in one atomic; a lowering after it queues v again,
+        // and pushing an older, larger colour meanwhile is harmless)
+        unsigned long long pv = 0;
+        int32_t rt = 0;
+        int64_t deg = 0, base = 0;
+        if (lane < nb) {
+            pv = KIND == 0 ? atomicOr(cc + v, 1ull) : __ldcg(cc + v);
+            if (KIND == 1) rt = __ldcg(rootof + v);
+            base = (int64_t)ld_off(beg, v);
+            deg = (int64_t)ld_off(beg, v + 1) - base;
+        }
+        int64_t incl = deg;
 #pragma unroll
-                    for (int q = 0; q < 4; ++q) w[q] = e + q < e1 ? ld_adj(adj, e + q) : -1;
-                    // one 8-byte load per neighbour carries its class and colour
-                    unsigned long long pw[4];
+        for (int o = 1; o < 32; o <<= 1) {
+            const int64_t t = __shfl_up_sync(kFull, incl, o);
+            if (lane >= o) incl += t;
+        }
+        const int64_t total = __shfl_sync(kFull, incl, 31);
+        base -= incl - deg;  // edge index of the chunk's k-th edge, k in this lane's range: base + k
+        for (int64_t k0 = 0; k0 < total; k0 += 64) {
+            int32_t w[2], vo[2];
+            unsigned long long po[2], pw[2];
+            int32_t ro[2];
 #pragma unroll
-                    for (int q = 0; q < 4; ++q) pw[q] = (w[q] >= 0 && w[q] != v) ? __ldcg(cc + w[q]) : 0ull;
-                    bool ok[4];
+            for (int u = 0; u < 2; ++u) {
+                const int64_t k = k0 + u * 32 + lane;
+                // owner: the number of lanes whose inclusive prefix is <= k
+                int o = 0;
 #pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        // the class compare also rejects inactive neighbours (dead class)
-                        ok[q] = w[q] >= 0 && w[q] != v && (pw[q] >> 32) == (pv >> 32);
-                        if (ok[q])
-                            ok[q] = KIND == 0 ? cv < colour_of(pw[q])
-                                              : (((pw[q] ^ pv) >> 1) == 0 && !bitv(r.F, w[q]));
+                for (int st = 16; st; st >>= 1)
+                    if (__shfl_sync(kFull, incl, o + st - 1) <= k) o += st;
+                const int64_t bo = __shfl_sync(kFull, base, o);
+                vo[u] = __shfl_sync(kFull, v, o);
+                po[u] = __shfl_sync(kFull, pv, o);
+                ro[u] = KIND == 1 ? __shfl_sync(kFull, rt, o) : 0;
+                w[u] = k < total ? ld_adj(adj, bo + k) : -1;
+            }
+#pragma unroll
+            for (int u = 0; u < 2; ++u) pw[u] = (w[u] >= 0 && w[u] != vo[u]) ? __ldcg(cc + w[u]) : 0ull;
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+                // the class compare also rejects inactive neighbours (dead class)
+                bool push = w[u] >= 0 && w[u] != vo[u] && (pw[u] >> 32) == (po[u] >> 32);
+                if (push) {
+                    if (KIND == 0) {
+                        const uint32_t cv = colour_of(po[u]);
+                        // lower the colour and clear the flag; the class cannot
+                        // change under a successful swap (it is compared first)
+                        const unsigned long long nw = (po[u] & 0xffffffff00000000ull) | ((unsigned long long)cv << 1);
+                        unsigned long long old = pw[u];
+                        bool lowered = false;
+                        int t = 0;
+                        // every failed swap saw a lower colour or a pop's flag
+                        for (; t < (1 << 20); ++t) {
+                            if ((old >> 32) != (po[u] >> 32) || colour_of(old) <= cv) break;
+                            const unsigned long long seen = atomicCAS(cc + w[u], old, nw);
+                            if (seen == old) { lowered = true; break; }
+                            old = seen;
+                        }
+                        if (t == (1 << 20)) atomicCAS(r.err, 0, kErrOverflow);
+                        push = lowered && (old & 1ull);  // the flag was set: not queued yet
+                    } else {
+                        push = ((pw[u] ^ po[u]) >> 1) == 0 && !bitv(r.F, w[u]) && set_bit(r.F, w[u]);
+                        if (push) rootof[w[u]] = ro[u];
                     }
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        if (!ok[q]) continue;
-                        if (KIND == 0) {
-                            // lower the colour and clear the flag; the class cannot
-                            // change under a successful swap (it is compared first)
-                            const unsigned long long nw = (pv & 0xffffffff00000000ull) | ((unsigned long long)cv << 1);
-                            unsigned long long old = pw[q];
-                            bool lowered = false;
-                            int t = 0;
-                            // every failed swap saw a lower colour or a pop's flag
-                            for (; t < (1 << 20); ++t) {
-                                if ((old >> 32) != (pv >> 32) || colour_of(old) <= cv) break;
-                                const unsigned long long seen = atomicCAS(cc + w[q], old, nw);
-                                if (seen == old) { lowered = true; break; }
-                                old = seen;
-                            }
-                            if (t == (1 << 20)) atomicCAS(r.err, 0, kErrOverflow);
-                            if (!lowered || !(old & 1ull)) continue;  // not lowered, or already queued
-                        } else {
-                            if (!set_bit(r.F, w[q])) continue;
-                            rootof[w[q]] = rt;
-                        }
-                        const int pos = atomicAdd(&sm.cnt[c ^ 1], 1);
-                        if (pos < kCLQ) {
-                            sm.lq[c ^ 1][pos] = w[q];
-                        } else {
-                            unsigned long long gp = atomicAdd(n_out, 1ull);
-                            if (VOK((long long)gp, 18)) q_out[gp] = w[q];
-                        }
+                }
+                const unsigned m = __ballot_sync(kFull, push);
+                if (m) {
+                    const int cnt = __popc(m), rank = __popc(m & lt);
+                    if (kCWQ - (tail - head) >= cnt) {
+                        if (push) ring[(tail + rank) & (kCWQ - 1)] = w[u];
+                        tail += cnt;
+                    } else {
+                        unsigned long long g = 0;
+                        if (lane == 0) g = atomicAdd(n_out, (unsigned long long)cnt);
+                        g = __shfl_sync(kFull, g, 0);
+                        if (push && VOK((long long)(g + rank), 18)) q_out[g + rank] = w[u];
                     }
                 }
             }
-            __syncthreads();
-            if (it + 1 >= r.color_levels) {
-                // Enough local levels this grid round: the frontier and the
-                // unread rest of the slice go back to the grid queue, so no
-                // CTA keeps the others waiting at the grid barrier; the next
-                // round spreads them over all CTAs.
-                const int m = min(sm.cnt[c ^ 1], kCLQ);
-                const int64_t rest = s1 - next_in;
-                if (tid == 0) sm.base = atomicAdd(n_out, (unsigned long long)(m + rest));
-                __syncthreads();
-                const unsigned long long b0 = sm.base;
-                for (int i = tid; i < m; i += kBlock)
-                    if (VOK((long long)(b0 + i), 18)) q_out[b0 + i] = sm.lq[c ^ 1][i];
-                for (int64_t i = tid; i < rest; i += kBlock)
-                    if (VOK((long long)(b0 + m + i), 18)) q_out[b0 + m + i] = __ldcg(q_in + next_in + i);
-                break;
-            }
-            if (tid == 0) {
-                const int m = min(sm.cnt[c ^ 1], kCLQ);
-                const int take = (int)min((int64_t)(kCLQ - m), s1 - next_in);
-                sm.cnt[c ^ 1] = m + take;
-                sm.take = take;
-                sm.cnt[c] = 0;
-            }
-            __syncthreads();
-            {
-                const int take = sm.take, m = sm.cnt[c ^ 1] - take;
-                for (int i = tid; i < take; i += kBlock) sm.lq[c ^ 1][m + i] = __ldcg(q_in + next_in + i);
-                next_in += take;
-            }
-            __syncthreads();
-            c ^= 1;
         }
+        __syncwarp();  // ring appends are visible to the warp's next chunk
+    }
+    if (capped && tail != head) {  // the ring goes back to the grid queue
+        const int cnt = tail - head;
+        unsigned long long g = 0;
+        if (lane == 0) g = atomicAdd(n_out, (unsigned long long)cnt);
+        g = __shfl_sync(kFull, g, 0);
+        for (int i = lane; i < cnt; i += 32)
+            if (VOK((long long)(g + i), 18)) q_out[g + i] = ring[(head + i) & (kCWQ - 1)];
+    }
+    __syncthreads();
+    // the unread rest of the slice (left by warps that reached their chunk cap)
+    const int64_t from = min((int64_t)sm.cursor, s1), rest = s1 - from;
+    if (rest > 0) {
+        __shared__ unsigned long long s_base;
+        if (threadIdx.x == 0) s_base = atomicAdd(n_out, (unsigned long long)rest);
+        __syncthreads();
+        const unsigned long long b0 = s_base;
+        for (int64_t i = threadIdx.x; i < rest; i += kBlock)
+            if (VOK((long long)(b0 + i), 18)) q_out[b0 + i] = __ldcg(q_in + from + i);
     }
 }
 
