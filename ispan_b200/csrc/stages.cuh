@@ -929,12 +929,31 @@ constexpr unsigned long long kDeadWord = ~0ull;        // class 0xffffffff: outs
 __device__ __forceinline__ uint32_t colour_of(unsigned long long w) { return ((uint32_t)w) >> 1; }
 
 constexpr int kCWQ = 256;     // per-warp frontier ring (entries); a power of two
+constexpr int kCPool = 1024;  // CTA work pool (entries); a power of two
 constexpr int kCLevels = 32;  // default of Run::color_levels: a warp works up to 4 * color_levels chunks of 32 entries per grid round
 constexpr int kCPivots = 1024;  // default of Run::color_pivots: pivots of the first colouring round
 struct ColorSmem {
     int32_t ring[kWarps][kCWQ];
+    int32_t pool[kCPool];
     unsigned long long cursor;  // next unread entry of this CTA's slice of the grid queue
+    int phead, ptail;           // pool entries [phead, ptail); guarded by lock
+    int active;                 // warps working (not waiting for pool work); guarded by lock
+    int lock;
 };
+
+// CTA spin lock in shared memory, taken by one lane.  Holders keep it for a
+// few shared-memory operations; the wait is bounded all the same.
+__device__ __forceinline__ void cta_lock(int *l, int *err) {
+    for (int i = 0; atomicCAS(l, 0, 1) != 0; ++i) {
+        if (i == (1 << 24)) { atomicCAS(err, 0, kErrTimeout); break; }
+        __nanosleep(32);
+    }
+    __threadfence_block();
+}
+__device__ __forceinline__ void cta_unlock(int *l) {
+    __threadfence_block();
+    atomicExch(l, 0);
+}
 
 // One asynchronous round over the global queue q_in[0..n_in).  KIND 0
 // relaxes colours forward inside the class (push the smaller colour to
@@ -942,15 +961,18 @@ struct ColorSmem {
 // root's SCC backward inside its colour (claim in-neighbours in F).
 //
 // Every warp works on its own: it takes 32 entries at a time from its ring
-// in shared memory, or from the CTA's slice of the grid queue when the ring
-// is empty, spreads the chunk's edges evenly over its lanes (a warp prefix
-// sum over the degrees, each lane finding its edge's owner by a binary
-// search over the prefix), and appends the vertices it queues to its ring
-// (the grid queue when the ring is full).  No barrier between warps: a warp
-// with a long list or slow loads delays no other.  After 4 * color_levels
-// chunks a warp hands its ring back to the grid queue, and the CTA hands
-// back the unread rest of its slice, so no CTA keeps the grid barrier
-// waiting; the next grid round spreads that work over all CTAs.
+// in shared memory, else from the CTA's slice of the grid queue, else from
+// the CTA's pool; it spreads the chunk's edges evenly over its lanes (a warp
+// prefix sum over the degrees, each lane finding its edge's owner by a
+// binary search over the prefix) and appends the vertices it queues to its
+// ring -- or, once its ring holds a chunk and some warp waits for work, to
+// the pool (the grid queue when both are full).  No barrier between warps:
+// a warp with a long list or slow loads delays no other, and a warp that
+// runs dry takes over work another warp generated.  A warp leaves when it
+// has worked 4 * color_levels chunks (handing its ring back to the grid
+// queue) or when the pool is empty and no warp is working; the CTA then
+// hands back the unread rest of its slice and the pool, so no CTA keeps the
+// grid barrier waiting; the next grid round spreads that work over all CTAs.
 template <typename OffT, int KIND>
 __device__ __forceinline__ void color_async_round(const Run<OffT> &r, const Ext<OffT> &x, const int32_t *q_in,
                                                   int64_t n_in, int32_t *q_out, unsigned long long *n_out,
@@ -963,15 +985,21 @@ __device__ __forceinline__ void color_async_round(const Run<OffT> &r, const Ext<
     const unsigned lt = lanemask_lt();
     int32_t *ring = sm.ring[threadIdx.x >> 5];
     const int64_t s0 = n_in * blockIdx.x / gridDim.x, s1 = n_in * (blockIdx.x + 1) / gridDim.x;
-    __syncthreads();  // the previous round's readers of the cursor are done
-    if (threadIdx.x == 0) sm.cursor = (unsigned long long)s0;
+    __syncthreads();  // the previous round's readers of the shared state are done
+    if (threadIdx.x == 0) {
+        sm.cursor = (unsigned long long)s0;
+        sm.phead = 0;
+        sm.ptail = 0;
+        sm.active = kWarps;
+        sm.lock = 0;
+    }
     __syncthreads();
     int head = 0, tail = 0;  // ring [head, tail), warp-uniform
     const int cap = 4 * r.color_levels;
     bool capped = false;
     for (int chunk = 0;; ++chunk) {
         if (chunk >= cap) { capped = true; break; }
-        int nb;
+        int nb = 0;
         int32_t v = -1;
         if (tail != head) {
             nb = min(32, tail - head);
@@ -981,9 +1009,49 @@ __device__ __forceinline__ void color_async_round(const Run<OffT> &r, const Ext<
             unsigned long long g = 0;
             if (lane == 0) g = atomicAdd(&sm.cursor, 32ull);
             g = __shfl_sync(kFull, g, 0);
-            if ((int64_t)g >= s1) break;
-            nb = (int)min((int64_t)32, s1 - (int64_t)g);
-            if (lane < nb) v = __ldcg(q_in + g + lane);
+            if ((int64_t)g < s1) {
+                nb = (int)min((int64_t)32, s1 - (int64_t)g);
+                if (lane < nb) v = __ldcg(q_in + g + lane);
+            } else {
+                // the pool, waiting for work while another warp may still add some
+                int got = 0, pb = 0;
+                if (lane == 0) {
+                    bool idle = false;
+                    const uint64_t t0 = globaltimer();
+                    for (int it = 0;; ++it) {
+                        // test without the lock first: waiting warps poll, the lock
+                        // stays free for the warps that feed the pool
+                        if (!idle || ld_volatile_int(&sm.ptail) != ld_volatile_int(&sm.phead) ||
+                            ld_volatile_int(&sm.active) == 0) {
+                            cta_lock(&sm.lock, r.err);
+                            const int avail = sm.ptail - sm.phead;
+                            if (avail > 0) {  // keep the lock until the lanes have read the entries
+                                got = min(32, avail);
+                                pb = sm.phead;
+                                sm.phead += got;
+                                if (idle) sm.active += 1;
+                                break;
+                            }
+                            if (!idle) { sm.active -= 1; idle = true; }
+                            const bool done = sm.active == 0;
+                            cta_unlock(&sm.lock);
+                            if (done) break;
+                        }
+                        if ((it & 63) == 63 && (globaltimer() - t0 > kBarrierTimeoutNs || ld_volatile_int(r.err))) {
+                            atomicCAS(r.err, 0, kErrTimeout);
+                            break;
+                        }
+                        __nanosleep(64);
+                    }
+                }
+                got = __shfl_sync(kFull, got, 0);
+                if (got == 0) break;  // nothing left in this CTA for this round
+                pb = __shfl_sync(kFull, pb, 0);
+                nb = got;
+                if (lane < nb) v = sm.pool[(pb + lane) & (kCPool - 1)];
+                __syncwarp();
+                if (lane == 0) cta_unlock(&sm.lock);
+            }
         }
         __syncwarp();  // ring slots read above may be refilled below
         // the chunk's vertices: KIND 0 leaves the queue here (sets the flag and
@@ -1056,10 +1124,34 @@ __device__ __forceinline__ void color_async_round(const Run<OffT> &r, const Ext<
                 const unsigned m = __ballot_sync(kFull, push);
                 if (m) {
                     const int cnt = __popc(m), rank = __popc(m & lt);
-                    if (kCWQ - (tail - head) >= cnt) {
+                    bool placed = false;
+                    // one read, broadcast: the branch below must be warp-uniform
+                    const int act = __shfl_sync(kFull, ld_volatile_int(&sm.active), 0);
+                    if (tail - head >= 32 && act < kWarps) {
+                        // share: a warp is waiting for work
+                        int pt = -1;
+                        if (lane == 0) {
+                            cta_lock(&sm.lock, r.err);
+                            if (kCPool - (sm.ptail - sm.phead) >= cnt) pt = sm.ptail;
+                            else cta_unlock(&sm.lock);
+                        }
+                        pt = __shfl_sync(kFull, pt, 0);
+                        if (pt >= 0) {
+                            if (push) sm.pool[(pt + rank) & (kCPool - 1)] = w[u];
+                            __syncwarp();
+                            if (lane == 0) {
+                                sm.ptail = pt + cnt;
+                                cta_unlock(&sm.lock);
+                            }
+                            placed = true;
+                        }
+                    }
+                    if (!placed && kCWQ - (tail - head) >= cnt) {
                         if (push) ring[(tail + rank) & (kCWQ - 1)] = w[u];
                         tail += cnt;
-                    } else {
+                        placed = true;
+                    }
+                    if (!placed) {
                         unsigned long long g = 0;
                         if (lane == 0) g = atomicAdd(n_out, (unsigned long long)cnt);
                         g = __shfl_sync(kFull, g, 0);
@@ -1070,24 +1162,35 @@ __device__ __forceinline__ void color_async_round(const Run<OffT> &r, const Ext<
         }
         __syncwarp();  // ring appends are visible to the warp's next chunk
     }
-    if (capped && tail != head) {  // the ring goes back to the grid queue
-        const int cnt = tail - head;
-        unsigned long long g = 0;
-        if (lane == 0) g = atomicAdd(n_out, (unsigned long long)cnt);
-        g = __shfl_sync(kFull, g, 0);
-        for (int i = lane; i < cnt; i += 32)
-            if (VOK((long long)(g + i), 18)) q_out[g + i] = ring[(head + i) & (kCWQ - 1)];
+    if (capped) {
+        if (lane == 0) {  // no longer working: waiting warps may leave
+            cta_lock(&sm.lock, r.err);
+            sm.active -= 1;
+            cta_unlock(&sm.lock);
+        }
+        if (tail != head) {  // the ring goes back to the grid queue
+            const int cnt = tail - head;
+            unsigned long long g = 0;
+            if (lane == 0) g = atomicAdd(n_out, (unsigned long long)cnt);
+            g = __shfl_sync(kFull, g, 0);
+            for (int i = lane; i < cnt; i += 32)
+                if (VOK((long long)(g + i), 18)) q_out[g + i] = ring[(head + i) & (kCWQ - 1)];
+        }
     }
     __syncthreads();
-    // the unread rest of the slice (left by warps that reached their chunk cap)
+    // the unread rest of the slice (left by warps that reached their chunk
+    // cap) and what is left in the pool go back to the grid queue
     const int64_t from = min((int64_t)sm.cursor, s1), rest = s1 - from;
-    if (rest > 0) {
+    const int pn = sm.ptail - sm.phead;
+    if (rest + pn > 0) {
         __shared__ unsigned long long s_base;
-        if (threadIdx.x == 0) s_base = atomicAdd(n_out, (unsigned long long)rest);
+        if (threadIdx.x == 0) s_base = atomicAdd(n_out, (unsigned long long)(rest + pn));
         __syncthreads();
         const unsigned long long b0 = s_base;
         for (int64_t i = threadIdx.x; i < rest; i += kBlock)
             if (VOK((long long)(b0 + i), 18)) q_out[b0 + i] = __ldcg(q_in + from + i);
+        for (int i = threadIdx.x; i < pn; i += kBlock)
+            if (VOK((long long)(b0 + rest + i), 18)) q_out[b0 + rest + i] = sm.pool[(sm.phead + i) & (kCPool - 1)];
     }
 }
 
