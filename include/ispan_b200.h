@@ -108,7 +108,8 @@ typedef struct {
     int64_t async_e;          /* ... and this many frontier edges (262144) */
     int32_t async_deg;        /* an asynchronous CTA expands vertices up to this degree itself (16) */
     int32_t bfs_ctas_per_sm;  /* CTAs per SM of the persistent searches, at most the occupancy limit (2) */
-    int32_t color_levels;     /* local levels a CTA works per grid round when colouring large WCCs (32) */
+    int32_t color_levels;     /* colouring large WCCs: a warp works up to 4 * color_levels chunks of 32
+                                 frontier entries per grid round before handing the rest back (32) */
     int32_t color_pivots;     /* about this many pivots in the first colouring round; doubles per round (1024) */
 } ispan_tuning;
 

@@ -4,10 +4,11 @@ Tuned: the push/pull switch of the reachability searches (alpha, beta, gamma:
 the reference's own knobs, src/fw_bw.h:576-624, whose defaults 30/200/10 come
 from src/bash_one.sh:4), the frontier sizes and vertex degree below which a
 search runs asynchronously inside CTAs (async_v, async_e, async_deg), and
-the CTAs per SM of the persistent searches (bfs_ctas_per_sm), the local
-levels a CTA works per grid round when colouring large WCCs (color_levels:
-fewer levels balance the CTAs, more save grid barriers) and the pivots of the
-colouring's first round (color_pivots).  None of them changes a label; they
+the CTAs per SM of the persistent searches (bfs_ctas_per_sm), the work a
+warp does per grid round when colouring large WCCs (color_levels: up to
+4 * color_levels chunks of 32 frontier entries; less balances the CTAs, more
+saves grid barriers) and the pivots of the colouring's first round
+(color_pivots).  None of them changes a label; they
 only move time between stages.
 
 Method: coordinate descent from the defaults over a small grid per

@@ -68,7 +68,7 @@ struct Run {
     uint32_t flags;
     int64_t async_v, async_e;     // a search goes asynchronous below these frontier sizes
     int32_t async_deg;            // degree up to which an asynchronous CTA expands a vertex itself
-    int32_t color_levels;         // local levels a CTA works per grid round of the colouring searches
+    int32_t color_levels;         // colouring: a warp works up to 4 * color_levels chunks of 32 entries per grid round
     int32_t color_pivots;         // about this many pivots in the first colouring round
 };
 
