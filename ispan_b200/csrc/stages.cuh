@@ -909,10 +909,10 @@ __global__ void __launch_bounds__(kLocalThreads) k_local_scc(Run<OffT> r, Ext<Of
 // the class compare also rejects inactive neighbours.
 //
 // Both searches run as asynchronous rounds: each CTA takes a slice of the
-// global frontier and works it to exhaustion with a frontier in shared
-// memory (levels separated by __syncthreads), overflowing to the global
-// queue; a grid barrier separates rounds, so ring-shaped SCCs cost no grid
-// barrier per hop.
+// global frontier, and its warps work it independently from frontier rings
+// in shared memory (a CTA pool passes work to warps that run dry),
+// overflowing to the global queue; a grid barrier separates rounds, so
+// ring-shaped SCCs cost no grid barrier per hop.
 __device__ __forceinline__ uint32_t prio_of(uint32_t v) {
     // bijection on [0, 2^31): xor-shifts and odd multipliers mod 2^31 are
     // invertible there
