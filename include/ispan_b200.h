@@ -246,7 +246,12 @@ int ispan_shard_expand(const ispan_csr *rows, int64_t v0, int64_t V, const uint8
  * The first call on a device resolves the array's address (no allocation);
  * make that first call before any stream capture.  All calls on a device
  * share the one array: calls that overlap on the GPU (different streams,
- * no ordering between them) race and must not be issued. */
+ * no ordering between them) race and must not be issued.  The kernel checks
+ * the graph before using any index read from it (offsets monotone from 0 to
+ * E, every id in [0, V)); a malformed graph gets -1 in every label (valid
+ * labels are never negative) and nothing past its arrays is touched.  An
+ * error already pending on the calling thread is returned as ISPAN_ERR_CUDA
+ * without clearing it and without a launch. */
 int ispan_scc_small_noalloc(const ispan_csr *g, int32_t *labels_out, void *stream);
 
 /* Reference-convention per-vertex codes from canonical labels and the class

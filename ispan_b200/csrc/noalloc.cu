@@ -13,7 +13,9 @@
 // thread of one CTA over the whole graph, with its per-vertex stacks in the
 // static scratch instead of shared memory; the other threads initialise the
 // scratch.  Labels are the minimum vertex id of each SCC, as from
-// ispan_scc_run.
+// ispan_scc_run.  The kernel first checks the graph (offsets monotone from 0
+// to E, ids in [0, V)) and answers a malformed one with -1 labels, so a bad
+// id can never index past the scratch.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -41,7 +43,7 @@ std::mutex g_setup_mu;
 
 template <typename OffT>
 __global__ void __launch_bounds__(256) k_scc_small_static(const OffT *__restrict__ fw_beg,
-                                                          const int32_t *__restrict__ fw_adj, int64_t V,
+                                                          const int32_t *__restrict__ fw_adj, int64_t V, int64_t E,
                                                           int32_t *__restrict__ labels, unsigned char *scratch) {
     int32_t *idx = reinterpret_cast<int32_t *>(scratch);
     int32_t *low = idx + kMaxV;
@@ -49,6 +51,24 @@ __global__ void __launch_bounds__(256) k_scc_small_static(const OffT *__restrict
     int32_t *csv = stk + kMaxV;
     int64_t *cse = reinterpret_cast<int64_t *>(csv + kMaxV);
     unsigned char *onst = reinterpret_cast<unsigned char *>(cse + kMaxV);
+    // Input check before any index taken from the graph is used: offsets
+    // monotone from 0 to E, every adjacency id in [0, V).  These loops read
+    // only fw_beg[0..V] and fw_adj[0..E), the arrays the caller declared.  A
+    // malformed graph gets -1 in every label and nothing else is touched (the
+    // Tarjan below indexes the scratch with adjacency ids).
+    int bad = 0;
+    for (int64_t v = threadIdx.x; v <= V; v += blockDim.x) {
+        const int64_t a = (int64_t)fw_beg[v];
+        if ((v == 0 && a != 0) || (v == V && a != E) || (v < V && (int64_t)fw_beg[v + 1] < a)) bad = 1;
+    }
+    for (int64_t e = threadIdx.x; e < E; e += blockDim.x) {
+        const int32_t w = fw_adj[e];
+        if (w < 0 || w >= V) bad = 1;
+    }
+    if (__syncthreads_or(bad)) {
+        for (int64_t v = threadIdx.x; v < V; v += blockDim.x) labels[v] = -1;
+        return;
+    }
     // the scratch keeps the last call's contents: reset what must start clear
     for (int64_t v = threadIdx.x; v < V; v += blockDim.x) {
         idx[v] = -1;
@@ -141,12 +161,16 @@ extern "C" int ispan_scc_small_noalloc(const ispan_csr *g, int32_t *labels_out, 
         }
         scratch = g_scratch_addr[dev];
     }
+    // an error left pending by earlier work on this thread is reported, not
+    // cleared, and no launch is made
+    if (cudaPeekAtLastError() != cudaSuccess) return ISPAN_ERR_CUDA;
     cudaStream_t s = (cudaStream_t)stream;
     if (g->offset_bytes == 4)
-        k_scc_small_static<int32_t><<<1, 256, 0, s>>>((const int32_t *)g->fw_beg, g->fw_adj, g->V, labels_out,
-                                                       (unsigned char *)scratch);
+        k_scc_small_static<int32_t><<<1, 256, 0, s>>>((const int32_t *)g->fw_beg, g->fw_adj, g->V, g->E,
+                                                       labels_out, (unsigned char *)scratch);
     else
-        k_scc_small_static<int64_t><<<1, 256, 0, s>>>((const int64_t *)g->fw_beg, g->fw_adj, g->V, labels_out,
-                                                       (unsigned char *)scratch);
+        k_scc_small_static<int64_t><<<1, 256, 0, s>>>((const int64_t *)g->fw_beg, g->fw_adj, g->V, g->E,
+                                                       labels_out, (unsigned char *)scratch);
+    // nothing was pending before the launch, so this is the launch's own status
     return cudaGetLastError() == cudaSuccess ? ISPAN_OK : ISPAN_ERR_CUDA;
 }

@@ -942,13 +942,16 @@ struct ColorSmem {
 };
 
 // CTA spin lock in shared memory, taken by one lane.  Holders keep it for a
-// few shared-memory operations; the wait is bounded all the same.
-__device__ __forceinline__ void cta_lock(int *l, int *err) {
+// few shared-memory operations; the wait is bounded all the same.  Returns
+// whether the lock was taken: on a timeout the error word is set and the
+// caller skips its critical section (and must not unlock).
+__device__ __forceinline__ bool cta_lock(int *l, int *err) {
     for (int i = 0; atomicCAS(l, 0, 1) != 0; ++i) {
-        if (i == (1 << 24)) { atomicCAS(err, 0, kErrTimeout); break; }
+        if (i == (1 << 24)) { atomicCAS(err, 0, kErrTimeout); return false; }
         __nanosleep(32);
     }
     __threadfence_block();
+    return true;
 }
 __device__ __forceinline__ void cta_unlock(int *l) {
     __threadfence_block();
@@ -1023,7 +1026,7 @@ __device__ __forceinline__ void color_async_round(const Run<OffT> &r, const Ext<
                         // stays free for the warps that feed the pool
                         if (!idle || ld_volatile_int(&sm.ptail) != ld_volatile_int(&sm.phead) ||
                             ld_volatile_int(&sm.active) == 0) {
-                            cta_lock(&sm.lock, r.err);
+                            if (!cta_lock(&sm.lock, r.err)) break;  // error recorded; this warp stops
                             const int avail = sm.ptail - sm.phead;
                             if (avail > 0) {  // keep the lock until the lanes have read the entries
                                 got = min(32, avail);
@@ -1130,8 +1133,7 @@ __device__ __forceinline__ void color_async_round(const Run<OffT> &r, const Ext<
                     if (tail - head >= 32 && act < kWarps) {
                         // share: a warp is waiting for work
                         int pt = -1;
-                        if (lane == 0) {
-                            cta_lock(&sm.lock, r.err);
+                        if (lane == 0 && cta_lock(&sm.lock, r.err)) {
                             if (kCPool - (sm.ptail - sm.phead) >= cnt) pt = sm.ptail;
                             else cta_unlock(&sm.lock);
                         }
@@ -1163,8 +1165,7 @@ __device__ __forceinline__ void color_async_round(const Run<OffT> &r, const Ext<
         __syncwarp();  // ring appends are visible to the warp's next chunk
     }
     if (capped) {
-        if (lane == 0) {  // no longer working: waiting warps may leave
-            cta_lock(&sm.lock, r.err);
+        if (lane == 0 && cta_lock(&sm.lock, r.err)) {  // no longer working: waiting warps may leave
             sm.active -= 1;
             cta_unlock(&sm.lock);
         }

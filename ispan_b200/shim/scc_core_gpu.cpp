@@ -62,12 +62,30 @@ void scc_detection(const graph *g, const int alpha, const int beta, const int ga
     ispan_stats st = {};
     int rc = ispan_scc_run(g_ctx, &c, &p, labels.data(), &st);
     if (rc) die("ispan_scc_run", rc);
-    const int slots[] = {0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 13};
-    for (int s : slots) avg_time[s] += st.stage_ms[s] / 1000.0;
-    printf("\ntime size_1, %.3lf\ntime pivot, %.3lf\nlargest fw, %.3lf\nlargest bw, %.3lf\ntrim size_2, %.3lf\n"
-           "trim size_3, %.3lf\nwcc time, %.3lf\nmice scc time, %.3lf\ntotal time, %.3lf\n",
-           st.stage_ms[4], st.stage_ms[6], st.stage_ms[7], st.stage_ms[8], st.stage_ms[5], st.stage_ms[13],
-           st.stage_ms[9], st.stage_ms[10], st.stage_ms[3]);
+    // Stage times in the reference's slots (src/scc_core.cpp:1037-1053) and
+    // its twelve per-run lines (src/scc_core.cpp:1062-1068), same keys and
+    // order.  The pivot keys are computed inside the trim-1-first pass, whose
+    // time is slot 6 of the engine's stage_ms; it is reported once, as
+    // "time size_1_first", and the pivot line reads 0.
+    const double *ms = st.stage_ms;
+    const double first = ms[6], size1 = ms[4] - ms[6], pivot = 0.0;
+    avg_time[0] += (ms[4] + ms[5] + ms[13]) / 1000.0;
+    avg_time[1] += (ms[7] + ms[8] + pivot) / 1000.0;
+    avg_time[2] += (ms[9] + ms[10]) / 1000.0;
+    avg_time[3] += ms[3] / 1000.0;
+    avg_time[4] += (first + size1) / 1000.0;
+    avg_time[5] += ms[5] / 1000.0;
+    avg_time[6] += pivot / 1000.0;
+    avg_time[7] += ms[7] / 1000.0;
+    avg_time[8] += ms[8] / 1000.0;
+    avg_time[9] += ms[9] / 1000.0;
+    avg_time[10] += ms[10] / 1000.0;
+    avg_time[13] += ms[13] / 1000.0;
+    printf("\ntime size_1_first, %.3lf\ntime size_1, %.3lf\ntime pivot, %.3lf\nlargest fw, %.3lf\n"
+           "largest bw, %.3lf\nlargest fw/bw, %.3lf\ntrim size_2, %.3lf\ntrim size_3, %.3lf\nwcc time, %.3lf\n"
+           "mice fw-bw time, %.3lf\nmice scc time, %.3lf\ntotal time, %.3lf\n",
+           first, size1, pivot, ms[7], ms[8], pivot + ms[7] + ms[8], ms[5], ms[13], ms[9], ms[10], ms[9] + ms[10],
+           ms[3]);
     std::vector<int32_t> codes((size_t)V + 1);
     rc = ispan_ref_codes(g_ctx, codes.data());
     if (rc) die("ispan_ref_codes", rc);

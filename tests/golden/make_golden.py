@@ -2,7 +2,7 @@
 
 Run where the reference tree is present (it is read at build time only):
 
-    make -C oracle ref && python tests/golden/make_golden.py
+    make -C oracle ref && python tests/golden/make_golden.py [--rmat16]
 
 For every fixture graph this writes ``<name>.npz`` holding the CSR, the raw
 per-vertex ``scc_id`` codes that the reference's unmodified CLI
@@ -13,6 +13,13 @@ labels from the independent Tarjan oracle.  ``ref_exact_t1`` /
 ``ref_exact_t4`` record whether the reference's answer, after splitting its
 codes into induced SCCs, equals the exact partition (it does not on some
 planted-cycle graphs: stale forward marks in init_fw_sa, src/fw_bw.h:1560).
+
+The plain-pipeline small workload (R-MAT scale 16, edge factor 16,
+(a,b,c) = (.57,.19,.19), self-loops and duplicates removed, seeds 1-10) gets
+its fixtures in ``rmat16/s<seed>.npz``: the graph is regenerated from its seed
+by ispan_b200.graphs.rmat (the fixture keeps a SHA-256 of its arrays to prove
+it is the same graph) and only the reference's raw codes (1 and 16 OpenMP
+threads) and its printed class report are stored.
 """
 from __future__ import annotations
 
@@ -50,6 +57,32 @@ def fixtures():
     yield "corners", G.from_edges(16, np.array(e))
 
 
+CONFIG1_SEEDS = range(1, 11)
+
+
+def csr_digest(csr):
+    import hashlib
+    h = hashlib.sha256()
+    for a in (csr.fw_beg, csr.fw_adj, csr.bw_beg, csr.bw_adj):
+        h.update(np.ascontiguousarray(a, np.int32).tobytes())
+    return h.hexdigest()
+
+
+def config1(tmp):
+    os.makedirs(os.path.join(HERE, "rmat16"), exist_ok=True)
+    for seed in CONFIG1_SEEDS:
+        csr = G.rmat(16, 16, seed)
+        exact = oracle.tarjan(csr)
+        out = dict(V=csr.V, E=csr.E, seed=seed, sha256=csr_digest(csr))
+        for t in (1, 16):
+            codes, report = run_cli(csr, os.path.join(tmp, f"rmat16_{seed}"), t)
+            out[f"ref_codes_t{t}"] = codes
+            out[f"ref_exact_t{t}"] = bool((oracle.canon_codes(csr, codes) == exact).all())
+            out[f"ref_report_t{t}"] = report
+        np.savez_compressed(os.path.join(HERE, "rmat16", f"s{seed}.npz"), **out)
+        print("rmat16", seed, csr.V, csr.E, "ref exact t1/t16:", out["ref_exact_t1"], out["ref_exact_t16"])
+
+
 def run_cli(csr, d, threads):
     paths = G.write_bin(csr, d)
     dump = os.path.join(d, "sid.bin")
@@ -66,6 +99,9 @@ def main():
     if not os.path.exists(oracle.REF_DUMP):
         sys.exit("build the reference first: make -C oracle ref")
     with tempfile.TemporaryDirectory() as tmp:
+        if "--rmat16" in sys.argv:
+            config1(tmp)
+            return
         for name, csr in fixtures():
             exact = oracle.tarjan(csr)
             out = dict(V=csr.V, E=csr.E, fw_beg=csr.fw_beg, fw_adj=csr.fw_adj,

@@ -131,3 +131,21 @@ def test_tuning_does_not_change_labels(tun):
                 assert np.array_equal(labels, oracle.tarjan(g))
         t = c.tuning()
         assert t["async_deg"] == tun["async_deg"]
+
+
+RMAT16 = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "rmat16", "s*.npz")))
+
+
+@pytest.mark.parametrize("path", RMAT16, ids=[os.path.basename(p)[:-4] for p in RMAT16])
+def test_rmat16_against_reference_fixture(ctx, path):
+    """The plain-pipeline small workload (R-MAT scale 16, edge factor 16,
+    seeds 1-10): GPU labels equal the reference's own OpenMP answer (its raw
+    codes from tests/golden/rmat16, canonicalised) and the exact partition."""
+    z = np.load(path)
+    csr = G.rmat(16, 16, int(z["seed"]))
+    assert csr.E == int(z["E"])
+    st = check(ctx, csr)
+    ref = oracle.canon_codes(csr, z["ref_codes_t16"])
+    labels, _ = ctx.run_csr(csr)
+    assert np.array_equal(labels, ref)
+    assert st["giant_size"] == int((z["ref_codes_t16"][:csr.V] == 1).sum())

@@ -107,3 +107,41 @@ def test_live_reference_matches_restatement():
         assert np.array_equal(sid, codes)
         sid4, _ = oracle.ref_run(csr, 4)
         assert np.array_equal(oracle.canon_codes(csr, sid4), oracle.tarjan(csr))
+
+
+# ---- the plain-pipeline small workload at full size: R-MAT scale 16, edge
+# factor 16, seeds 1-10, pinned to the reference's own CLI (golden/rmat16/)
+RMAT16 = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "rmat16", "s*.npz")))
+
+
+def rmat16(path):
+    """The fixture's graph, regenerated from its seed and checked against the
+    digest the fixture recorded."""
+    import importlib.util
+    z = np.load(path)
+    csr = G.rmat(16, 16, int(z["seed"]))
+    spec = importlib.util.spec_from_file_location(
+        "make_golden", os.path.join(os.path.dirname(__file__), "golden", "make_golden.py"))
+    mg = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mg)
+    assert mg.csr_digest(csr) == str(z["sha256"]), "regenerated graph differs from the fixture's"
+    return csr, z
+
+
+def test_rmat16_fixtures_present():
+    assert len(RMAT16) == 10
+
+
+@pytest.mark.parametrize("path", RMAT16, ids=[os.path.basename(p)[:-4] for p in RMAT16])
+def test_rmat16_restatement_and_reference(path):
+    csr, z = rmat16(path)
+    exact = oracle.tarjan(csr)
+    # the serial restatement with the reference's quirks emits its serial codes
+    _, codes, _ = oracle.ispan(csr, quirks=oracle.QUIRKS_ALL)
+    assert np.array_equal(codes, z["ref_codes_t1"])
+    # the reference is exact on these graphs at 1 and 16 threads
+    for t in (1, 16):
+        assert bool(z[f"ref_exact_t{t}"])
+        assert np.array_equal(oracle.canon_codes(csr, z[f"ref_codes_t{t}"]), exact)
+    labels, _, _ = oracle.ispan(csr)
+    assert np.array_equal(labels, exact)
