@@ -66,12 +66,17 @@ typedef struct {
 #define ISPAN_F_NO_L2_WINDOW 8u     /* no persisting L2 window over the status maps */
 #define ISPAN_F_VALIDATE 16u        /* check a device-resident CSR before the run
                                        (host CSRs are always checked) */
-#define ISPAN_F_EXACT_STATS 32u     /* also fill fw_edges / bw_edges (one extra pass) */
+#define ISPAN_F_EXACT_STATS 32u     /* also fill fw_edges / bw_edges and the trims' worklist
+                                       sizes (extra passes) */
 
 /* Stage-time slots follow the reference's avg_time[15] meanings
  * (src/scc_core.cpp:24-25, :1037-1053): 0 trim, 1 elephant SCC, 2 mice SCC,
- * 3 total, 4 trim size_1, 5 trim size_2, 6 pivot selection, 7 FW, 8 BW,
- * 9 WCC, 10 mice FW-BW, 13 trim size_3.  Milliseconds of device time. */
+ * 3 total, 4 trim size_1, 5 trim size_2, 6 pivot selection (fused with the
+ * first trim-1 pass here), 7 FW, 8 BW, 9 WCC, 10 mice FW-BW, 13 trim size_3.
+ * Finer slots without a reference counterpart: 11 colouring of the large
+ * WCCs (part of 10), 12 second trim-1 peel, 14 residual worklist after the
+ * pivot SCCs, 15 first trim-1 peel (12, 14, 15 are parts of 4).
+ * Milliseconds of device time. */
 typedef struct {
     double stage_ms[16];
     int64_t scc_count;        /* number of SCCs (no phantom vertex, unlike Q1) */
@@ -85,6 +90,12 @@ typedef struct {
      * size; the caller supplies the arrays (hist_cap entries) or NULLs */
     int64_t *hist_size, *hist_count;
     int64_t hist_cap, hist_n;
+    /* worklists of the trims (ISPAN_F_EXACT_STATS): the peel's input is the
+     * residual after the pivot SCCs (`residual` vertices, sum of their out-
+     * plus in-degrees resid_edges); trim-2/3 read the peel's survivors */
+    int64_t resid_edges;
+    int64_t peeled_residual;       /* vertices left after the first peel */
+    int64_t peeled_residual_edges; /* sum of their out- plus in-degrees */
 } ispan_stats;
 
 typedef struct ispan_ctx ispan_ctx;
@@ -156,23 +167,35 @@ int ispan_graphs_run(ispan_ctx *ctx, const ispan_csr *gs, int32_t n, int32_t *co
                      const ispan_params *p, ispan_stats *st);
 
 /* ---- served form: continuous batching over a request queue ------------
- * No counterpart in the reference (one graph per process).  A server owns
- * n_slots batch slots (a context each, the budget split between them) and a
- * worker thread per slot.  Requests are served in arrival order; a slot takes
- * the queued requests that fit when the device is idle or a full batch is
- * waiting, packs them while another slot's batch runs, and runs when the
- * device frees (one pipeline on the device at a time).  A request's graph and
- * label buffer must stay valid until the request is reported done. */
+ * No counterpart in the reference (one graph per process).  A server runs
+ * n_slots lanes, each a context with its own CUDA stream and worker thread,
+ * concurrently on one GPU.  A lane whose batch is done takes its share of
+ * the queued requests (arrival order) at once, while the other lanes'
+ * batches are still running, so a request that arrives while others are on
+ * the GPU is admitted as soon as a lane and memory free up and its work
+ * overlaps theirs on the device.  Memory: the budget is one device
+ * allocation made at creation; each batch's exact footprint (pipeline
+ * scratch, union CSR and tables for its vertex, edge and graph counts) is
+ * taken from it when the batch is admitted and returned when its labels are
+ * written; a batch that does not fit the free memory waits.  A request's
+ * graph and label buffer must stay valid until the request is reported
+ * done. */
 typedef struct ispan_server ispan_server;
 
 typedef struct {
     int32_t device;
     int32_t max_batch_graphs;   /* graphs per batch; 0: 4096 */
-    int32_t n_slots;            /* batch slots (contexts) sharing the budget; 0: 2 */
+    int32_t n_slots;            /* lanes running batches concurrently; 0: 4.  With
+                                   more than one, each lane's persistent stages use
+                                   0.9 / n_slots of the SMs */
     int32_t reserved;
-    int64_t hbm_budget_bytes;   /* device memory the server may hold; 0: 64 GiB */
-    int64_t max_batch_V;        /* vertices / edges per batch (one slot); 0: the */
-    int64_t max_batch_E;        /*   largest at 16 edges per vertex within the slot's share */
+    int64_t hbm_budget_bytes;   /* device memory the server holds (allocated at
+                                   creation); 0: 64 GiB */
+    int64_t max_batch_V;        /* vertices / edges of a batch of several graphs; 0:
+                                   the largest */
+    int64_t max_batch_E;        /*   at 16 edges per vertex in budget / n_slots.  A
+                                   single larger request runs alone if its footprint
+                                   fits the budget */
     int64_t max_wait_us;        /* a partial batch waits this long for more requests */
     int64_t max_pending;        /* queued requests before submit returns ISPAN_ERR_BUSY; 0: no limit */
     ispan_params params;
@@ -183,26 +206,29 @@ typedef struct {
     int32_t batch_graphs;    /* graphs in the batch that served it */
     int64_t batch_id;
     int64_t t_submit_ns;     /* CLOCK_MONOTONIC */
-    int64_t t_start_ns;      /* its batch started packing */
+    int64_t t_start_ns;      /* its batch was admitted (set while it runs) */
     int64_t t_done_ns;       /* its labels were written */
 } ispan_request_info;
 
-/* Fails with ISPAN_ERR_NOMEM when the explicit batch size does not fit the
- * budget. */
+/* Fails with ISPAN_ERR_NOMEM when the budget cannot be allocated or the
+ * explicit batch size does not fit it. */
 int ispan_server_create(const ispan_server_config *cfg, ispan_server **out);
 int ispan_server_limits(const ispan_server *s, int64_t *max_V, int64_t *max_E, int32_t *max_graphs);
 /* Queue one graph (host or device CSR); labels_out[g->V] (host or device)
- * receives its local min-id labels.  A graph larger than one batch is refused
- * with ISPAN_ERR_CAPACITY. */
+ * receives its local min-id labels.  A graph whose footprint exceeds the
+ * whole budget is refused with ISPAN_ERR_CAPACITY. */
 int ispan_server_submit(ispan_server *s, const ispan_csr *g, int32_t *labels_out, int64_t *ticket);
 /* 1 done, 0 not yet, or the request's error; a finished request is reported
  * once (a second poll of its ticket returns ISPAN_ERR_ARG). */
 int ispan_server_poll(ispan_server *s, int64_t ticket, ispan_request_info *info);
 /* As poll, blocking up to timeout_us (negative: no limit); 0 on timeout. */
 int ispan_server_wait(ispan_server *s, int64_t ticket, int64_t timeout_us, ispan_request_info *info);
-/* batches, graphs, vertices, edges served, busy ns, queued requests */
+/* Up to n of: batches, graphs, vertices, edges served; busy ns (wall time
+ * with at least one batch in flight); queued requests; lane ns (sum of the
+ * batches' wall times: lane ns / busy ns is the mean number of batches in
+ * flight); budget bytes in use; peak budget bytes in use; lanes. */
 int ispan_server_counters(ispan_server *s, int64_t *out, int32_t n);
-/* Serves what is queued, then stops the worker and frees the device memory. */
+/* Serves what is queued, then stops the lanes and frees the device memory. */
 int ispan_server_destroy(ispan_server *s);
 
 /* Condensation: the DAG of the SCCs of a device-resident graph g (only its

@@ -218,8 +218,10 @@ class Context:
 
 class Server:
     """Served form (ispan_server_* of include/ispan_b200.h): submit graphs one
-    at a time; a worker thread batches whatever is queued into one disjoint
-    union per batch.  Each request's arrays and label buffer must stay alive
+    at a time; ``n_slots`` lanes (default 4) take the queued requests as they
+    free up and run their batches (one disjoint union each) concurrently on
+    the GPU, each batch's memory taken from the ``hbm_budget_bytes`` budget
+    while it runs.  Each request's arrays and label buffer must stay alive
     until the request is reported done (the object keeps references)."""
 
     def __init__(self, device=0, hbm_budget_bytes=0, max_batch_graphs=0, max_batch_V=0, max_batch_E=0,
@@ -232,6 +234,7 @@ class Server:
         check(_lib.lib().ispan_server_create(C.byref(cfg), C.byref(h)), "ispan_server_create")
         self._h = h
         self._keep: dict = {}
+        self._done: dict = {}  # finished requests seen by peek()
 
     def limits(self):
         v, e, n = C.c_int64(), C.c_int64(), C.c_int32()
@@ -251,34 +254,54 @@ class Server:
 
     def poll(self, ticket: int):
         """None while queued or running, else the request's info dict."""
+        if ticket in self._done:
+            return self._finish(ticket, *self._done.pop(ticket))
         info = _lib.RequestInfo()
         rc = _lib.lib().ispan_server_poll(self._h, ticket, C.byref(info))
         if rc == 0:
             return None
-        self._keep.pop(ticket, None)
-        check(rc if rc < 0 else 0, "request %d" % ticket)
-        return info.as_dict()
+        return self._finish(ticket, rc, info.as_dict())
+
+    def peek(self, ticket: int) -> dict:
+        """The request's info without consuming it: status 0 while queued or
+        running (t_start_ns is set once its batch is admitted)."""
+        if ticket in self._done:
+            return dict(self._done[ticket][1])
+        info = _lib.RequestInfo()
+        rc = _lib.lib().ispan_server_poll(self._h, ticket, C.byref(info))
+        d = info.as_dict()
+        if rc != 0:  # finished: the library reported it once; keep it for poll/wait
+            self._done[ticket] = (rc, d)
+        return dict(d)
 
     def wait(self, ticket: int, timeout_s: float | None = None):
+        if ticket in self._done:
+            return self._finish(ticket, *self._done.pop(ticket))
         info = _lib.RequestInfo()
         us = -1 if timeout_s is None else int(timeout_s * 1e6)
         rc = _lib.lib().ispan_server_wait(self._h, ticket, us, C.byref(info))
         if rc == 0:
             return None
+        return self._finish(ticket, rc, info.as_dict())
+
+    def _finish(self, ticket, rc, info):
         self._keep.pop(ticket, None)
         check(rc if rc < 0 else 0, "request %d" % ticket)
-        return info.as_dict()
+        return info
 
     def counters(self) -> dict:
-        out = np.zeros(6, np.int64)
-        check(_lib.lib().ispan_server_counters(self._h, out.ctypes.data, 6), "counters")
-        return dict(zip(("batches", "graphs", "vertices", "edges", "busy_ns", "queued"), (int(x) for x in out)))
+        keys = ("batches", "graphs", "vertices", "edges", "busy_ns", "queued", "lane_ns", "bytes_in_use",
+                "bytes_peak", "lanes")
+        out = np.zeros(len(keys), np.int64)
+        check(_lib.lib().ispan_server_counters(self._h, out.ctypes.data, len(keys)), "counters")
+        return dict(zip(keys, (int(x) for x in out)))
 
     def close(self) -> None:
         if getattr(self, "_h", None):
             _lib.lib().ispan_server_destroy(self._h)
             self._h = None
             self._keep.clear()
+            self._done.clear()
 
     def __del__(self):
         try:
@@ -385,8 +408,8 @@ def scc_detection(g: graph, alpha: int, beta: int, gamma: int, theta: float, thr
     ctx = _context_for(g.vert_count, g.edge_count)
     labels, st = ctx.run(g.fw_beg_pos, g.fw_csr, g.bw_beg_pos, g.bw_csr, V=g.vert_count, alpha=alpha,
                          beta=beta, gamma=gamma, theta=theta, stage_times=True)
-    for i, ms in enumerate(st["stage_ms"][:15]):
-        avg_time[i] += ms / 1000.0
+    for i in (0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 13):  # the reference's slots only
+        avg_time[i] += st["stage_ms"][i] / 1000.0
     codes = ctx.ref_codes(g.vert_count)
     (result_hook or get_scc_result)(codes, g.vert_count)
     return labels

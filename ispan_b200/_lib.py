@@ -50,7 +50,8 @@ class Stats(C.Structure):
         "scc_count", "giant_size", "n_trim1", "n_trim2", "n_trim3", "n_mice_vertices", "n_mice_scc", "n_wcc",
         "fw_size", "fw_levels", "bw_levels", "residual", "color_rounds", "local_wcc", "trim_rounds",
         "fw_edges", "bw_edges")] + [
-        ("hist_size", C.c_void_p), ("hist_count", C.c_void_p), ("hist_cap", C.c_int64), ("hist_n", C.c_int64)]
+        ("hist_size", C.c_void_p), ("hist_count", C.c_void_p), ("hist_cap", C.c_int64), ("hist_n", C.c_int64),
+        ("resid_edges", C.c_int64), ("peeled_residual", C.c_int64), ("peeled_residual_edges", C.c_int64)]
 
     def as_dict(self) -> dict:
         d = {k: getattr(self, k) for k, _ in self._fields_ if k not in ("stage_ms", "hist_size", "hist_count")}

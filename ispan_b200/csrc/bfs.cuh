@@ -588,4 +588,23 @@ __global__ void __launch_bounds__(kBlock) k_reach_degrees(Run<OffT> r) {
     }
 }
 
+// Size and out+in degree sum of a worklist (statistics only, on request):
+// the algorithmic bytes of the trim stages that read it.
+template <typename OffT>
+__global__ void __launch_bounds__(kBlock) k_list_degrees(Run<OffT> r, const int32_t *wl,
+                                                         const unsigned long long *n_wl, int slot_n, int slot_deg) {
+    __shared__ int64_t sh[kWarps];
+    const int64_t n = (int64_t)*n_wl;
+    int64_t d = 0;
+    for (int64_t i = (int64_t)blockIdx.x * kBlock + threadIdx.x; i < n; i += (int64_t)gridDim.x * kBlock) {
+        const int64_t v = wl[i];
+        d += ld_off(r.fw_beg, v + 1) - ld_off(r.fw_beg, v) + ld_off(r.bw_beg, v + 1) - ld_off(r.bw_beg, v);
+    }
+    const int64_t t = block_sum64(d, sh);
+    if (threadIdx.x == 0) {
+        if (t) atomicAdd(r.counters + slot_deg, (unsigned long long)t);
+        if (slot_n >= 0 && blockIdx.x == 0) r.counters[slot_n] = (unsigned long long)n;
+    }
+}
+
 }  // namespace ispan

@@ -96,6 +96,9 @@ enum Counter {
     C_SPILL,         // small WCCs whose edges overflowed shared memory
     C_FW_XDEG,       // sum of out-degrees over F  (algorithmic bytes of the FW search)
     C_BW_XDEG,       // sum of in-degrees over S   (algorithmic bytes of the BW search)
+    C_Q1_XDEG,       // sum of out+in degrees over the peel's worklist (residual after the giant)
+    C_Q2_N,          // vertices left after the first peel (trim-2/3 worklist)
+    C_Q2_XDEG,       // sum of their out+in degrees
     kNumCounters = 32
 };
 constexpr int kHistCap = 1 << 16;   // exact histogram for SCC sizes below this

@@ -26,6 +26,7 @@
 #include "bfs.cuh"
 #include "pack.cuh"
 #include "stages.cuh"
+#include "lane.h"
 
 using namespace ispan;
 
@@ -41,9 +42,24 @@ namespace {
         }                                                                            \
     } while (0)
 
+// A context's scratch comes from cudaMalloc, or -- for a server lane -- is
+// carved out of a region of the server's device-memory budget.  A region
+// with a null base only measures (the footprint of a carve).
+struct Region {
+    char *base = nullptr;
+    size_t cap = 0, used = 0;
+};
+
 template <typename T>
-static int dalloc(T **p, size_t n, std::vector<void *> &owned) {
+static int dalloc(T **p, size_t n, std::vector<void *> &owned, Region *rg = nullptr) {
     if (n == 0) n = 1;
+    if (rg) {
+        const size_t at = (rg->used + 255) / 256 * 256, bytes = n * sizeof(T);
+        if (rg->base && at + bytes > rg->cap) return ISPAN_ERR_NOMEM;
+        *p = rg->base ? (T *)(rg->base + at) : nullptr;
+        rg->used = at + bytes;
+        return ISPAN_OK;
+    }
     void *q = nullptr;
     if (cudaMalloc(&q, n * sizeof(T)) != cudaSuccess) {
         cudaGetLastError();
@@ -63,11 +79,16 @@ __global__ void k_barrier_probe(unsigned *gs, int *err, uint64_t limit_ns) {
     grid_sync(gs, err, limit_ns);
 }
 
+constexpr int kNumEv = 13;  // stage boundaries recorded per run
+
 }  // namespace
 
 struct ispan_ctx {
     int device = 0;
     int nsm = 148;
+    int nsm_coop = 0;               // SMs the persistent grids are sized for (0: all)
+    Region *rg = nullptr;           // scratch carved from a server's budget (lanes)
+    Region lane_region;             // the region rg points to while a lane is bound
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     int64_t maxV = 0, maxE = 0, maxW = 0;
@@ -93,7 +114,9 @@ struct ispan_ctx {
     PackDesc *h_desc = nullptr;                    // pinned mirrors
     int64_t *h_vbeb = nullptr;                     // pinned [2 * (pk_n + 1)]
     int64_t pk_n = 0;
-    std::vector<void *> pk_owned;
+    int64_t h_cap = 0;                             // entries of the pinned mirrors
+    std::vector<void *> pk_owned;                  // union buffers
+    std::vector<void *> pkt_owned;                 // per-graph tables
     std::vector<int64_t> pk_vbase;  // segmentation of the packed union
     int64_t pk_cur_n = 0, pk_Et = 0;
     bool pk_ready = false;          // a packed union waits for its run
@@ -133,7 +156,7 @@ struct ispan_ctx {
     cudaGraphExec_t gexec = nullptr;
     char gkey[256];
     bool graph_broken = false;
-    cudaEvent_t ev[12];
+    cudaEvent_t ev[kNumEv];
     bool have_ev = false;
 
     // last run (for ispan_ref_codes)
@@ -172,11 +195,12 @@ static int ctx_alloc(ispan_ctx *c) {
     c->maxW = W;
     int rc = 0;
     auto &o = c->owned;
-    rc |= dalloc(&c->label, V, o);
-    rc |= dalloc(&c->cls, V, o);
+    Region *g = c->rg;
+    rc |= dalloc(&c->label, V, o, g);
+    rc |= dalloc(&c->cls, V, o, g);
     // the six status maps in one block, so one L2 access-policy window covers them
     const int64_t Wp = (W + 63) / 64 * 64;  // 256-byte aligned slices
-    rc |= dalloc(&c->bits, 6 * Wp, o);
+    rc |= dalloc(&c->bits, 6 * Wp, o, g);
     c->bits_bytes = 6 * Wp * 4;
     if (!rc) {
         c->A = c->bits;
@@ -187,39 +211,40 @@ static int ctx_alloc(ispan_ctx *c) {
         c->T = c->bits + 5 * Wp;
     }
     for (int i = 0; i < 2; ++i) {
-        rc |= dalloc(&c->qv[i], V, o);
-        rc |= dalloc(&c->qe[i], V + 1, o);
-        rc |= dalloc(&c->qchunk[i], E / kChunk + 4, o);
-        rc |= dalloc(&c->wl[i], V, o);
-        rc |= dalloc(&c->large[i], V, o);
+        rc |= dalloc(&c->qv[i], V, o, g);
+        rc |= dalloc(&c->qe[i], V + 1, o, g);
+        rc |= dalloc(&c->qchunk[i], E / kChunk + 4, o, g);
+        rc |= dalloc(&c->wl[i], V, o, g);
+        rc |= dalloc(&c->large[i], V, o, g);
     }
-    rc |= dalloc(&c->cnt_out, V, o);
-    rc |= dalloc(&c->cnt_in, V, o);
-    rc |= dalloc(&c->parent, V, o);
-    rc |= dalloc(&c->aux, V, o);
-    rc |= dalloc(&c->aux2, V, o);
-    rc |= dalloc(&c->members, V, o);
-    rc |= dalloc(&c->roots, V, o);
-    rc |= dalloc(&c->small, V, o);
-    rc |= dalloc(&c->ctlblk, kCtlTotal, o);
-    rc |= dalloc(&c->hist, kHistCap + kBigCap, o);
-    rc |= dalloc(&c->gsync, 4, o);
-    rc |= dalloc(&c->err, 4, o);
-    rc |= dalloc(&c->bfsctl, 1, o);
-    rc |= dalloc(&c->trace, 3 * kTraceLevels * 4, o);
+    rc |= dalloc(&c->cnt_out, V, o, g);
+    rc |= dalloc(&c->cnt_in, V, o, g);
+    rc |= dalloc(&c->parent, V, o, g);
+    rc |= dalloc(&c->aux, V, o, g);
+    rc |= dalloc(&c->aux2, V, o, g);
+    rc |= dalloc(&c->members, V, o, g);
+    rc |= dalloc(&c->roots, V, o, g);
+    rc |= dalloc(&c->small, V, o, g);
+    rc |= dalloc(&c->ctlblk, kCtlTotal, o, g);
+    rc |= dalloc(&c->hist, kHistCap + kBigCap, o, g);
+    rc |= dalloc(&c->gsync, 4, o, g);
+    rc |= dalloc(&c->err, 4, o, g);
+    rc |= dalloc(&c->bfsctl, 1, o, g);
+    rc |= dalloc(&c->trace, 3 * kTraceLevels * 4, o, g);
     return rc ? ISPAN_ERR_NOMEM : ISPAN_OK;
 }
 
 static int ctx_segments(ispan_ctx *c, int64_t nseg) {
     if (nseg <= c->maxSeg) return ISPAN_OK;
+    if (c->rg && c->maxSeg > 0) return ISPAN_ERR_CAPACITY;  // a lane's tables were carved for its batch
     for (void *p : c->seg_owned) cudaFree(p);
     c->seg_owned.clear();
     int64_t n = std::max<int64_t>(nseg, 1);
     int rc = 0;
-    rc |= dalloc(&c->vbase, n + 1, c->seg_owned);
-    rc |= dalloc(&c->pivot_key, n, c->seg_owned);
-    rc |= dalloc(&c->gsize, n, c->seg_owned);
-    rc |= dalloc(&c->gmin, n, c->seg_owned);
+    rc |= dalloc(&c->vbase, n + 1, c->seg_owned, c->rg);
+    rc |= dalloc(&c->pivot_key, n, c->seg_owned, c->rg);
+    rc |= dalloc(&c->gsize, n, c->seg_owned, c->rg);
+    rc |= dalloc(&c->gmin, n, c->seg_owned, c->rg);
     if (rc) {
         c->maxSeg = 0;
         return ISPAN_ERR_NOMEM;
@@ -338,8 +363,10 @@ static cudaError_t enqueue(ispan_ctx *c, Run<OffT> r, Ext<OffT> x, bool times, b
     if (r.flags & ISPAN_F_EXACT_STATS) LK((k_reach_degrees<OffT><<<G, kBlock, 0, s>>>(r)));
     EV(3);
     LK((k_giant_residual<OffT><<<G, kBlock, 0, s>>>(r, x)));
+    if (r.flags & ISPAN_F_EXACT_STATS) LK((k_list_degrees<OffT><<<G, kBlock, 0, s>>>(r, r.wl[0], x.ctl + K_WL0, -1, C_Q1_XDEG)));
     EV(4);
     if ((e = launch_coop(k_trim1<OffT>, c->g_coop[2], s, r, x, 0, 1))) return e;
+    if (r.flags & ISPAN_F_EXACT_STATS) LK((k_list_degrees<OffT><<<G, kBlock, 0, s>>>(r, r.wl[1], x.ctl + K_WL1, C_Q2_N, C_Q2_XDEG)));
     EV(5);
     LK((k_trim2<OffT><<<G, kBlock, 0, s>>>(r, x, 1)));
     EV(6);
@@ -356,10 +383,11 @@ static cudaError_t enqueue(ispan_ctx *c, Run<OffT> r, Ext<OffT> x, bool times, b
     LK((k_wcc_scatter<OffT><<<G, kBlock, 0, s>>>(r, x, 0)));
     EV(9);
     LK((k_local_scc<OffT><<<c->nsm * 6, kLocalThreads, 0, s>>>(r, x)));
-    if ((e = launch_coop(k_color<OffT>, c->g_coop[3], s, r, x))) return e;
     EV(10);
-    LK((k_finalize<OffT><<<G, kBlock, 0, s>>>(r, x)));
+    if ((e = launch_coop(k_color<OffT>, c->g_coop[3], s, r, x))) return e;
     EV(11);
+    LK((k_finalize<OffT><<<G, kBlock, 0, s>>>(r, x)));
+    EV(12);
 #undef EV
 #undef LK
     return cudaSuccess;
@@ -369,14 +397,17 @@ template <typename OffT>
 static int coop_setup(ispan_ctx *c) {
     int w = (int)sizeof(OffT);
     if (c->g_coop_w == w) return ISPAN_OK;
-    c->g_coop[0] = coop_grid(k_bfs<OffT, 0>, c->nsm, kBlock);
-    c->g_coop[1] = coop_grid(k_bfs<OffT, 1>, c->nsm, kBlock);
+    // a server lane sizes its persistent grids for its share of the SMs, so
+    // the lanes' persistent kernels are co-resident whatever runs at once
+    const int nsm = c->nsm_coop > 0 ? c->nsm_coop : c->nsm;
+    c->g_coop[0] = coop_grid(k_bfs<OffT, 0>, nsm, kBlock);
+    c->g_coop[1] = coop_grid(k_bfs<OffT, 1>, nsm, kBlock);
     // fewer CTAs per SM than the occupancy limit on request (never more)
     const int want = c->tuning.bfs_ctas_per_sm;
     if (want > 0)
-        for (int i = 0; i < 2; ++i) c->g_coop[i] = std::min(c->g_coop[i], want * c->nsm);
-    c->g_coop[2] = coop_grid(k_trim1<OffT>, c->nsm, kBlock);
-    c->g_coop[3] = coop_grid(k_color<OffT>, c->nsm, kBlock);
+        for (int i = 0; i < 2; ++i) c->g_coop[i] = std::min(c->g_coop[i], want * nsm);
+    c->g_coop[2] = coop_grid(k_trim1<OffT>, nsm, kBlock);
+    c->g_coop[3] = coop_grid(k_color<OffT>, nsm, kBlock);
     for (int i = 0; i < 4; ++i)
         if (c->g_coop[i] < 1) return ISPAN_ERR_CUDA;
     c->g_coop_w = w;
@@ -533,25 +564,35 @@ static int run_t(ispan_ctx *c, int64_t V, int64_t E, int32_t nseg, const OffT *f
         st->residual = (int64_t)(k[C_ACTIVE0] - k[C_GIANT]);
         st->fw_edges = (int64_t)k[C_FW_XDEG];
         st->bw_edges = (int64_t)k[C_BW_XDEG];
+        st->resid_edges = (int64_t)k[C_Q1_XDEG];
+        st->peeled_residual = (int64_t)k[C_Q2_N];
+        st->peeled_residual_edges = (int64_t)k[C_Q2_XDEG];
         st->scc_count = (int64_t)(k[C_TRIM1] + k[C_TRIM2] / 2 + k[C_TRIM3] / 3 + k[C_MICE_SCC] + k[C_GIANTS]);
         if (times) {
-            float ms[12];
-            for (int i = 1; i < 12; ++i) cudaEventElapsedTime(&ms[i], c->ev[i - 1], c->ev[i]);
+            float ms[kNumEv];
+            for (int i = 1; i < kNumEv; ++i) cudaEventElapsedTime(&ms[i], c->ev[i - 1], c->ev[i]);
             // reference slots: 0 trim, 1 elephant, 2 mice, 3 total, 4 trim size_1,
-            // 5 trim size_2, 6 pivot, 7 fw, 8 bw, 9 wcc, 10 mice fw-bw, 13 trim size_3
+            // 5 trim size_2, 6 pivot, 7 fw, 8 bw, 9 wcc, 10 mice fw-bw, 13 trim size_3;
+            // finer slots of this engine: 11 large-WCC colouring (part of 10),
+            // 12 second peel, 14 residual worklist after the pivot SCCs, 15 first
+            // peel (12, 14 and 15 are parts of 4)
             st->stage_ms[6] = ms[1];
             st->stage_ms[7] = ms[2];
             st->stage_ms[8] = ms[3];
+            st->stage_ms[14] = ms[4];
+            st->stage_ms[15] = ms[5];
+            st->stage_ms[12] = ms[8];
             st->stage_ms[4] = ms[1] + ms[4] + ms[5] + ms[8];
             st->stage_ms[5] = ms[6];
             st->stage_ms[13] = ms[7];
             st->stage_ms[9] = ms[9];
-            st->stage_ms[10] = ms[10];
+            st->stage_ms[11] = ms[11];
+            st->stage_ms[10] = ms[10] + ms[11];
             st->stage_ms[0] = st->stage_ms[4] + st->stage_ms[5] + st->stage_ms[13];
             st->stage_ms[1] = ms[2] + ms[3];
-            st->stage_ms[2] = ms[9] + ms[10];
+            st->stage_ms[2] = st->stage_ms[9] + st->stage_ms[10];
             float tot = 0;
-            cudaEventElapsedTime(&tot, c->ev[0], c->ev[11]);
+            cudaEventElapsedTime(&tot, c->ev[0], c->ev[kNumEv - 1]);
             st->stage_ms[3] = tot;
         }
         st->hist_n = 0;
@@ -695,14 +736,16 @@ static int run_common(ispan_ctx *c, const ispan_csr *g, int32_t nseg, const int6
 }
 
 // union buffers for ispan_scc_run_graphs: the CSR at the context's capacity
-// on first use, the per-graph tables grown to n
+// on first use, the per-graph tables grown to n (device tables from the
+// lane's region when the context is bound to one; pinned host mirrors always
+// from cudaMallocHost)
 static int pk_reserve(ispan_ctx *c, int64_t n) {
     if (!c->pk_fwb) {
         int rc = 0;
-        rc |= dalloc(&c->pk_fwb, c->maxV + 1, c->pk_owned);
-        rc |= dalloc(&c->pk_bwb, c->maxV + 1, c->pk_owned);
-        rc |= dalloc(&c->pk_fwa, c->maxE, c->pk_owned);
-        rc |= dalloc(&c->pk_bwa, c->maxE, c->pk_owned);
+        rc |= dalloc(&c->pk_fwb, c->maxV + 1, c->pk_owned, c->rg);
+        rc |= dalloc(&c->pk_bwb, c->maxV + 1, c->pk_owned, c->rg);
+        rc |= dalloc(&c->pk_fwa, c->maxE, c->pk_owned, c->rg);
+        rc |= dalloc(&c->pk_bwa, c->maxE, c->pk_owned, c->rg);
         if (rc) {
             for (void *q : c->pk_owned) cudaFree(q);
             c->pk_owned.clear();
@@ -711,27 +754,31 @@ static int pk_reserve(ispan_ctx *c, int64_t n) {
             return ISPAN_ERR_NOMEM;
         }
     }
+    if (n > c->h_cap) {
+        const int64_t m = std::max<int64_t>({n, 2 * c->h_cap, 64});
+        if (c->h_desc) cudaFreeHost(c->h_desc);
+        if (c->h_vbeb) cudaFreeHost(c->h_vbeb);
+        c->h_desc = nullptr;
+        c->h_vbeb = nullptr;
+        c->h_cap = 0;
+        if (cudaMallocHost(&c->h_desc, m * sizeof(PackDesc)) != cudaSuccess ||
+            cudaMallocHost(&c->h_vbeb, 2 * (m + 1) * sizeof(int64_t)) != cudaSuccess) {
+            cudaGetLastError();
+            return ISPAN_ERR_NOMEM;
+        }
+        c->h_cap = m;
+    }
     if (n <= c->pk_n) return ISPAN_OK;
-    const int64_t m = std::max<int64_t>({n, 2 * c->pk_n, 64});
-    // the first four allocations above stay; drop the per-graph tables
-    std::vector<void *> keep(c->pk_owned.begin(), c->pk_owned.begin() + 4);
-    for (size_t i = 4; i < c->pk_owned.size(); ++i) cudaFree(c->pk_owned[i]);
-    c->pk_owned = keep;
-    if (c->h_desc) cudaFreeHost(c->h_desc);
-    if (c->h_vbeb) cudaFreeHost(c->h_vbeb);
-    c->h_desc = nullptr;
-    c->h_vbeb = nullptr;
+    if (c->rg && c->pk_n > 0) return ISPAN_ERR_CAPACITY;  // a lane's tables were carved for its batch
+    const int64_t m = c->rg ? std::max<int64_t>(n, 1) : std::max<int64_t>({n, 2 * c->pk_n, 64});
+    for (void *q : c->pkt_owned) cudaFree(q);
+    c->pkt_owned.clear();
     c->pk_n = 0;
     int rc = 0;
-    rc |= dalloc(&c->pk_desc, m, c->pk_owned);
-    rc |= dalloc(&c->pk_vb, 2 * (m + 1), c->pk_owned);
-    rc |= dalloc(&c->pk_stage, 2 * (c->maxV + m), c->pk_owned);
-    if (!rc && cudaMallocHost(&c->h_desc, m * sizeof(PackDesc)) != cudaSuccess) rc = ISPAN_ERR_NOMEM;
-    if (!rc && cudaMallocHost(&c->h_vbeb, 2 * (m + 1) * sizeof(int64_t)) != cudaSuccess) rc = ISPAN_ERR_NOMEM;
-    if (rc) {
-        cudaGetLastError();
-        return ISPAN_ERR_NOMEM;
-    }
+    rc |= dalloc(&c->pk_desc, m, c->pkt_owned, c->rg);
+    rc |= dalloc(&c->pk_vb, 2 * (m + 1), c->pkt_owned, c->rg);
+    rc |= dalloc(&c->pk_stage, 2 * (c->maxV + m), c->pkt_owned, c->rg);
+    if (rc) return ISPAN_ERR_NOMEM;
     c->pk_eb = c->pk_vb + (m + 1);
     c->pk_n = m;
     return ISPAN_OK;
@@ -870,6 +917,95 @@ static int run_graphs(ispan_ctx *c, const ispan_csr *gs, int32_t n, int32_t *con
     return rc ? rc : run_packed(c, gs, n, labels_out, p, st);
 }
 
+// ---------------------------------------------------------------------------
+// Server lanes (server.cu): a context whose scratch and union buffers are
+// carved, per batch, out of a region of the server's device-memory budget.
+
+// Carve every scratch array for a batch of n graphs with V vertices and E
+// edges in total; with a null base the region only measures.
+static int ctx_carve(ispan_ctx *c, int64_t V, int64_t E, int64_t n) {
+    c->maxV = V;
+    c->maxE = E;
+    c->maxSeg = 0;
+    c->pk_fwb = c->pk_bwb = nullptr;
+    c->pk_fwa = c->pk_bwa = nullptr;
+    c->pk_n = 0;
+    c->pk_ready = false;
+    int rc = ctx_alloc(c);
+    if (!rc) rc = ctx_segments(c, std::max<int64_t>(n, 1));
+    if (!rc) rc = pk_reserve(c, std::max<int64_t>(n, 1));
+    return rc;
+}
+
+size_t lane_region_bytes(int64_t V, int64_t E, int64_t n) {
+    ispan_ctx m;
+    Region r;  // null base: measure only
+    m.rg = &r;
+    m.h_cap = INT64_MAX;  // no pinned mirrors for a measurement
+    ctx_carve(&m, V, E, n);
+    m.rg = nullptr;
+    return r.used + 256;
+}
+
+int lane_bind(ispan_ctx *c, void *base, size_t bytes, int64_t V, int64_t E, int64_t n) {
+    std::lock_guard<std::mutex> lock(c->mu);
+    if (cudaSetDevice(c->device) != cudaSuccess) return ISPAN_ERR_CUDA;
+    Region &r = c->lane_region;
+    r.base = (char *)base;
+    r.cap = bytes;
+    r.used = (size_t)((256 - ((uintptr_t)base & 255)) & 255);
+    c->rg = &r;
+    if (c->gexec) {  // the captured graph holds the previous batch's pointers
+        cudaGraphExecDestroy(c->gexec);
+        c->gexec = nullptr;
+    }
+    c->vbase_host.clear();
+    c->g_coop_w = 0;
+    const int rc = ctx_carve(c, V, E, n);
+    if (rc) {
+        c->rg = nullptr;
+        c->maxV = c->maxE = 0;
+    }
+    return rc;
+}
+
+void lane_unbind(ispan_ctx *c) {
+    std::lock_guard<std::mutex> lock(c->mu);
+    c->rg = nullptr;
+    c->maxV = c->maxE = c->maxSeg = 0;  // nothing runs on a lane between batches
+    c->pk_fwb = c->pk_bwb = nullptr;
+    c->pk_fwa = c->pk_bwa = nullptr;
+    c->pk_n = 0;
+    c->pk_ready = false;
+    c->last_V = 0;
+}
+
+int lane_set_sm_share(ispan_ctx *c, int nsm) {
+    std::lock_guard<std::mutex> lock(c->mu);
+    c->nsm_coop = std::max(1, std::min(nsm, c->nsm));
+    c->g_coop_w = 0;
+    return ISPAN_OK;
+}
+
+// pinned host mirrors for batches of up to n graphs, allocated once per lane
+// (freeing pinned memory later would synchronise the device)
+int lane_reserve_host(ispan_ctx *c, int64_t n) {
+    std::lock_guard<std::mutex> lock(c->mu);
+    if (n <= c->h_cap) return ISPAN_OK;
+    if (c->h_desc) cudaFreeHost(c->h_desc);
+    if (c->h_vbeb) cudaFreeHost(c->h_vbeb);
+    c->h_desc = nullptr;
+    c->h_vbeb = nullptr;
+    c->h_cap = 0;
+    if (cudaMallocHost(&c->h_desc, n * sizeof(PackDesc)) != cudaSuccess ||
+        cudaMallocHost(&c->h_vbeb, 2 * (n + 1) * sizeof(int64_t)) != cudaSuccess) {
+        cudaGetLastError();
+        return ISPAN_ERR_NOMEM;
+    }
+    c->h_cap = n;
+    return ISPAN_OK;
+}
+
 extern "C" {
 
 int ispan_ctx_create(int device, int64_t max_V, int64_t max_E, ispan_ctx **out) {
@@ -895,7 +1031,7 @@ int ispan_ctx_create(int device, int64_t max_V, int64_t max_E, ispan_ctx **out) 
         rc = ISPAN_ERR_NOMEM;
     if (!rc && cudaMallocHost(&c->h_err, 4 * sizeof(int)) != cudaSuccess) rc = ISPAN_ERR_NOMEM;
     if (!rc) {
-        for (int i = 0; i < 12; ++i)
+        for (int i = 0; i < kNumEv; ++i)
             if (cudaEventCreate(&c->ev[i]) != cudaSuccess) rc = ISPAN_ERR_CUDA;
         c->have_ev = rc == 0;
     }
@@ -920,11 +1056,12 @@ int ispan_ctx_destroy(ispan_ctx *c) {
     for (void *p : c->seg_owned) cudaFree(p);
     for (void *p : c->csr_owned) cudaFree(p);
     for (void *p : c->pk_owned) cudaFree(p);
+    for (void *p : c->pkt_owned) cudaFree(p);
     if (c->h_desc) cudaFreeHost(c->h_desc);
     if (c->h_vbeb) cudaFreeHost(c->h_vbeb);
     if (c->l2_limit_set) cudaCtxResetPersistingL2Cache();
     if (c->have_ev)
-        for (int i = 0; i < 12; ++i) cudaEventDestroy(c->ev[i]);
+        for (int i = 0; i < kNumEv; ++i) cudaEventDestroy(c->ev[i]);
     if (c->h_counters) cudaFreeHost(c->h_counters);
     if (c->h_err) cudaFreeHost(c->h_err);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);

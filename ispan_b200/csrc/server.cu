@@ -1,22 +1,35 @@
-// server.cu -- served SCC detection: requests (one graph each) are queued,
-// gathered into batches while the device works on the previous batch
-// (continuous batching), and run as one disjoint union per batch through
-// the two phases of ispan_scc_run_graphs (ispan_graphs_pack, then
-// ispan_graphs_run).  Declared in include/ispan_b200.h (ispan_server_*).
+// server.cu -- served SCC detection with continuous batching.  Declared in
+// include/ispan_b200.h (ispan_server_*).
 //
 // The reference has no serving mode: it runs one graph per process
 // (src/scc_main.cpp:41-47).  Results are those of ispan_scc_run on the graph
-// alone: the union's segments never interact (edges stay inside their
-// graph, every segment gets its own pivot), and labels are translated back to
-// each graph's local ids.
+// alone: a batch is a disjoint union whose segments never interact (edges
+// stay inside their graph, every segment gets its own pivot), and labels are
+// translated back to each graph's local ids.
 //
-// Admission: the budget is split between the batch slots, each a context
-// plus its union buffers; a request larger than one batch is refused at
-// submission (ISPAN_ERR_CAPACITY), and the queue may be bounded
-// (ISPAN_ERR_BUSY).  Requests run in arrival order; a batch takes requests
-// from the head of the queue while they fit.  While one slot's batch runs,
-// another slot packs the next batch (host copies and the pack kernels on its
-// own stream), so arrivals join the device work as soon as a slot frees.
+// Lanes.  The server runs n_slots lanes, each a context with its own stream
+// and worker thread.  A lane whose previous batch is done takes the next
+// requests from the head of the queue at once -- while the other lanes'
+// batches are still on the device -- so requests that arrive while others
+// run are admitted as soon as a lane and memory free up, and their work
+// overlaps the running batches on the GPU.  Each lane's persistent stage
+// kernels are sized for its share of the SMs (lane.h), which keeps every
+// lane's persistent grid co-resident with the others'.
+//
+// Memory.  The device-memory budget is one allocation made at creation; a
+// batch's footprint (every scratch array of its pipeline, the union CSR and
+// its tables, exact to the byte for its vertex, edge and graph counts) is
+// carved out of it with a first-fit allocator when the batch is admitted and
+// handed back when its labels are written.  A request whose footprint alone
+// exceeds the budget is refused at submission (ISPAN_ERR_CAPACITY); a batch
+// that does not fit the free memory waits for running batches to finish.
+// No cudaMalloc or cudaFree runs while batches are in flight (both would
+// synchronise the whole device and stall the other lanes).
+//
+// Requests are taken in arrival order.  A lane takes its share of the queue
+// (the queued requests split over the idle lanes), at most max_batch_graphs
+// and the per-batch vertex and edge limits, shrunk until it fits the free
+// memory.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -25,12 +38,14 @@
 #include <cstdio>
 #include <cstring>
 #include <deque>
+#include <map>
 #include <mutex>
 #include <thread>
 #include <unordered_map>
 #include <vector>
 
 #include "../../include/ispan_b200.h"
+#include "lane.h"
 
 namespace {
 
@@ -46,62 +61,116 @@ struct Req {
     ispan_request_info info;
 };
 
-// device bytes of a server whose batches hold up to V vertices, E edges and
-// n graphs: the context plus the union CSR and its staging tables
-int64_t server_bytes(int64_t V, int64_t E, int64_t n) {
-    return ispan_ctx_bytes(V, E) + 2 * 8 * (V + 1) + 2 * 4 * E + 2 * 8 * (V + n) + 4 * 8 * (n + 1) + 96 * n;
-}
+// First-fit allocator over one device allocation (offsets 256-byte aligned);
+// adjacent free ranges are merged on release.
+struct Arena {
+    size_t cap = 0, used = 0, peak = 0;
+    std::map<size_t, size_t> free_;  // offset -> bytes
+
+    void init(size_t bytes) {
+        cap = bytes;
+        free_.clear();
+        free_[0] = bytes;
+    }
+    bool alloc(size_t bytes, size_t *off) {
+        bytes = (bytes + 255) / 256 * 256;
+        for (auto it = free_.begin(); it != free_.end(); ++it) {
+            if (it->second < bytes) continue;
+            *off = it->first;
+            const size_t rest = it->second - bytes;
+            const size_t at = it->first + bytes;
+            free_.erase(it);
+            if (rest) free_[at] = rest;
+            used += bytes;
+            peak = std::max(peak, used);
+            return true;
+        }
+        return false;
+    }
+    void release(size_t off, size_t bytes) {
+        bytes = (bytes + 255) / 256 * 256;
+        used -= bytes;
+        auto it = free_.emplace(off, bytes).first;
+        auto nx = std::next(it);
+        if (nx != free_.end() && it->first + it->second == nx->first) {
+            it->second += nx->second;
+            free_.erase(nx);
+        }
+        if (it != free_.begin()) {
+            auto pv = std::prev(it);
+            if (pv->first + pv->second == it->first) {
+                pv->second += it->second;
+                free_.erase(it);
+            }
+        }
+    }
+};
 
 }  // namespace
 
 struct ispan_server {
     ispan_server_config cfg;
-    std::vector<ispan_ctx *> ctx;   // one per batch slot
-    int64_t capV = 0, capE = 0;     // per batch (one slot)
+    int device = 0;
+    std::vector<ispan_ctx *> lanes;
+    int64_t capV = 0, capE = 0;     // per-batch limits when a batch holds more than one graph
     int32_t capN = 0;
+    char *dev_base = nullptr;       // the budget
+    Arena arena;
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
     std::deque<int64_t> pending;
     std::unordered_map<int64_t, Req> reqs;
     int64_t next_ticket = 1, next_batch = 0;
-    int64_t n_batches = 0, n_graphs = 0, n_vertices = 0, n_edges = 0, busy_ns = 0;
+    int64_t n_batches = 0, n_graphs = 0, n_vertices = 0, n_edges = 0;
+    int64_t busy_ns = 0;            // wall time with at least one lane's batch in flight
+    int64_t lane_ns = 0;            // sum over batches of their wall time
+    int64_t busy_since = 0;
+    int active = 0;                 // lanes with a batch in flight
+    int idle = 0;                   // lanes waiting for work
     bool stop = false;
-    bool device_busy = false;       // a slot's pipeline is on the device
-    std::mutex dev_mu;              // one pipeline on the device at a time
     std::vector<std::thread> workers;
+    ispan_params params;
 
-    bool batch_full() const {
-        int64_t v = 0, e = 0, k = 0;
+    // pack and run one batch on lane c inside its region
+    int pack_run(ispan_ctx *c, char *base, size_t bytes, std::vector<ispan_csr> &gs, std::vector<int32_t *> &labs) {
+        int64_t V = 0, E = 0;
+        for (const ispan_csr &g : gs) {
+            V += g.V;
+            E += g.E;
+        }
+        int rc = lane_bind(c, base, bytes, V, E, (int64_t)gs.size());
+        if (!rc) rc = ispan_graphs_pack(c, gs.data(), (int32_t)gs.size());
+        if (!rc) rc = ispan_graphs_run(c, gs.data(), (int32_t)gs.size(), labs.data(), &params, nullptr);
+        lane_unbind(c);
+        return rc;
+    }
+
+    // the head of the queue this lane takes: its share of the queued
+    // requests, within the batch limits, shrunk until it fits free memory;
+    // false when nothing can be admitted now
+    bool admit(std::vector<int64_t> &take, size_t *off, size_t *bytes) {
+        const int64_t share = ((int64_t)pending.size() + idle - 1) / std::max(1, idle);
+        int64_t v = 0, e = 0;
         for (int64_t t : pending) {
+            if ((int64_t)take.size() >= std::min<int64_t>(capN, std::max<int64_t>(share, 1))) break;
             const Req &r = reqs.at(t);
-            if (k + 1 > capN || v + r.g.V > capV || e + r.g.E > capE) return true;
+            if (!take.empty() && (v + r.g.V > capV || e + r.g.E > capE)) break;
             v += r.g.V;
             e += r.g.E;
-            ++k;
+            take.push_back(t);
+        }
+        while (!take.empty()) {
+            *bytes = lane_region_bytes(v, e, (int64_t)take.size());
+            if (arena.alloc(*bytes, off)) return true;
+            const Req &r = reqs.at(take.back());
+            v -= r.g.V;
+            e -= r.g.E;
+            take.pop_back();
         }
         return false;
     }
 
-    // pack on this slot's context (overlapping another slot's run), then run
-    // when the device is free
-    int pack_run(ispan_ctx *c, std::vector<ispan_csr> &gs, std::vector<int32_t *> &labs) {
-        int rc = ispan_graphs_pack(c, gs.data(), (int32_t)gs.size());
-        if (rc) return rc;
-        std::lock_guard<std::mutex> dev(dev_mu);
-        {
-            std::lock_guard<std::mutex> lk(mu);
-            device_busy = true;
-        }
-        rc = ispan_graphs_run(c, gs.data(), (int32_t)gs.size(), labs.data(), &cfg.params, nullptr);
-        {
-            std::lock_guard<std::mutex> lk(mu);
-            device_busy = false;
-        }
-        cv_work.notify_all();  // an idle device lets a waiting slot take a batch
-        return rc;
-    }
-
-    void run_batch(ispan_ctx *c, std::vector<int64_t> &take) {
+    void run_batch(ispan_ctx *c, std::vector<int64_t> &take, size_t off, size_t bytes, int64_t t0) {
         std::vector<ispan_csr> gs;
         std::vector<int32_t *> labs;
         {
@@ -112,31 +181,30 @@ struct ispan_server {
                 labs.push_back(r.labels);
             }
         }
-        const int64_t t0 = now_ns();
         std::vector<int> rcs(take.size(), 0);
-        int rc = pack_run(c, gs, labs);
+        int rc = pack_run(c, dev_base + off, bytes, gs, labs);
         if (rc == ISPAN_ERR_ARG && gs.size() > 1) {
-            // a malformed graph fails the whole union: run each alone so only
-            // that request reports the error
+            // a malformed graph fails the whole union: run each alone (its
+            // footprint is below the batch's) so only that request fails
             for (size_t i = 0; i < gs.size(); ++i) {
                 std::vector<ispan_csr> g1(1, gs[i]);
                 std::vector<int32_t *> l1(1, labs[i]);
-                rcs[i] = pack_run(c, g1, l1);
+                rcs[i] = pack_run(c, dev_base + off, bytes, g1, l1);
             }
         } else {
             std::fill(rcs.begin(), rcs.end(), rc);
         }
         const int64_t t1 = now_ns();
         std::lock_guard<std::mutex> lk(mu);
+        arena.release(off, bytes);
         const int64_t bid = next_batch++;
         ++n_batches;
-        busy_ns += t1 - t0;
+        lane_ns += t1 - t0;
+        if (--active == 0) busy_ns += t1 - busy_since;
         for (size_t i = 0; i < take.size(); ++i) {
             Req &r = reqs.at(take[i]);
             r.info.status = rcs[i] == 0 ? 1 : rcs[i];
             r.info.batch_id = bid;
-            r.info.batch_graphs = (int32_t)take.size();
-            r.info.t_start_ns = t0;
             r.info.t_done_ns = t1;
             if (rcs[i] == 0) {
                 ++n_graphs;
@@ -145,34 +213,47 @@ struct ispan_server {
             }
         }
         cv_done.notify_all();
+        cv_work.notify_all();  // memory was freed: a waiting lane may admit now
     }
 
-    // A slot takes a batch when the device is idle (latency) or a full batch
-    // is queued (throughput: it packs while the running batch computes).
-    void loop(int slot) {
-        ispan_ctx *c = ctx[slot];
+    void loop(int k) {
+        ispan_ctx *c = lanes[k];
         for (;;) {
             std::vector<int64_t> take;
+            size_t off = 0, bytes = 0;
+            int64_t t0 = 0;
             {
                 std::unique_lock<std::mutex> lk(mu);
-                cv_work.wait(lk, [&] { return stop || (!pending.empty() && (!device_busy || batch_full())); });
-                if (stop && pending.empty()) return;
-                if (cfg.max_wait_us > 0 && !stop) {
-                    // let a partial batch fill for a bounded time
-                    auto until = std::chrono::steady_clock::now() + std::chrono::microseconds(cfg.max_wait_us);
-                    cv_work.wait_until(lk, until, [&] { return stop || batch_full(); });
+                ++idle;
+                for (;;) {
+                    if (stop && pending.empty()) {
+                        --idle;
+                        return;
+                    }
+                    if (!pending.empty()) {
+                        if (cfg.max_wait_us > 0 && !stop && (int64_t)pending.size() < capN) {
+                            // let a partial batch fill for a bounded time
+                            auto until = std::chrono::steady_clock::now() + std::chrono::microseconds(cfg.max_wait_us);
+                            cv_work.wait_until(lk, until, [&] { return stop || (int64_t)pending.size() >= capN; });
+                            if (pending.empty()) continue;
+                        }
+                        take.clear();
+                        if (admit(take, &off, &bytes)) break;
+                    }
+                    cv_work.wait(lk);
                 }
-                int64_t v = 0, e = 0;
-                while (!pending.empty() && (int32_t)take.size() < capN) {
-                    const Req &r = reqs.at(pending.front());
-                    if (!take.empty() && (v + r.g.V > capV || e + r.g.E > capE)) break;
-                    v += r.g.V;
-                    e += r.g.E;
-                    take.push_back(pending.front());
-                    pending.pop_front();
+                --idle;
+                for (size_t i = 0; i < take.size(); ++i) pending.pop_front();
+                t0 = now_ns();
+                if (active++ == 0) busy_since = t0;
+                for (int64_t t : take) {
+                    Req &r = reqs.at(t);
+                    r.info.t_start_ns = t0;
+                    r.info.batch_graphs = (int32_t)take.size();
                 }
+                if (!pending.empty()) cv_work.notify_one();  // the rest is for another lane
             }
-            if (!take.empty()) run_batch(c, take);
+            run_batch(c, take, off, bytes, t0);
         }
     }
 };
@@ -182,25 +263,30 @@ extern "C" {
 int ispan_server_create(const ispan_server_config *cfg, ispan_server **out) {
     if (!cfg || !out) return ISPAN_ERR_ARG;
     *out = nullptr;
+    const int64_t budget = cfg->hbm_budget_bytes > 0 ? cfg->hbm_budget_bytes : (64ll << 30);
+    const int nl = cfg->n_slots > 0 ? cfg->n_slots : 4;
+    if (nl > 64) return ISPAN_ERR_ARG;
     ispan_server *s = new ispan_server();
     s->cfg = *cfg;
-    const int64_t budget = cfg->hbm_budget_bytes > 0 ? cfg->hbm_budget_bytes : (64ll << 30);
-    const int nslots = cfg->n_slots > 0 ? cfg->n_slots : 2;
-    const int64_t share = budget / nslots;
+    s->device = cfg->device;
+    s->params = cfg->params;
+    // each lane's L2 window would evict the others' maps; lanes run without
+    s->params.flags = (s->params.flags | ISPAN_F_NO_L2_WINDOW) & ~(uint32_t)ISPAN_F_LABELS_ON_DEVICE;
     s->capN = cfg->max_batch_graphs > 0 ? cfg->max_batch_graphs : 4096;
+    const int64_t share = budget / nl;  // per-batch size limit: a lane's share of the budget
     if (cfg->max_batch_V > 0 && cfg->max_batch_E >= 0) {
         s->capV = cfg->max_batch_V;
         s->capE = cfg->max_batch_E;
-        if (server_bytes(s->capV, s->capE, s->capN) > share) {
+        if ((int64_t)lane_region_bytes(s->capV, s->capE, s->capN) > budget) {
             delete s;
             return ISPAN_ERR_NOMEM;
         }
     } else {
-        // the largest batch at 16 edges per vertex that fits a slot's share
+        // the largest batch at 16 edges per vertex within a lane's share
         int64_t lo = 0, hi = (int64_t)INT32_MAX - 64;
         while (lo < hi) {
             int64_t mid = (lo + hi + 1) / 2;
-            if (server_bytes(mid, 16 * mid, s->capN) <= share) lo = mid; else hi = mid - 1;
+            if ((int64_t)lane_region_bytes(mid, 16 * mid, s->capN) <= share) lo = mid; else hi = mid - 1;
         }
         if (lo < 1024) {
             delete s;
@@ -209,17 +295,42 @@ int ispan_server_create(const ispan_server_config *cfg, ispan_server **out) {
         s->capV = lo;
         s->capE = 16 * lo;
     }
-    for (int k = 0; k < nslots; ++k) {
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        delete s;
+        return ISPAN_ERR_NODEV;
+    }
+    if (cfg->device < 0 || cfg->device >= ndev || cudaSetDevice(cfg->device) != cudaSuccess) {
+        delete s;
+        return ISPAN_ERR_ARG;
+    }
+    if (cudaMalloc(&s->dev_base, (size_t)budget) != cudaSuccess) {
+        cudaGetLastError();
+        delete s;
+        return ISPAN_ERR_NOMEM;
+    }
+    s->arena.init((size_t)budget);
+    int nsm = 148;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, cfg->device);
+    // one lane gets every SM; several share 90 % of them, the rest left as
+    // slack so the lanes' persistent grids always fit next to each other
+    const int sm_share = nl == 1 ? nsm : std::max(1, nsm * 9 / 10 / nl);
+    for (int k = 0; k < nl; ++k) {
         ispan_ctx *c = nullptr;
-        int rc = ispan_ctx_create(cfg->device, s->capV, s->capE, &c);
+        int rc = ispan_ctx_create(cfg->device, 0, 0, &c);
+        if (!rc) rc = lane_set_sm_share(c, sm_share);
+        if (!rc) rc = lane_reserve_host(c, s->capN);
         if (rc) {
-            for (ispan_ctx *d : s->ctx) ispan_ctx_destroy(d);
+            if (c) ispan_ctx_destroy(c);
+            for (ispan_ctx *d : s->lanes) ispan_ctx_destroy(d);
+            cudaFree(s->dev_base);
             delete s;
             return rc;
         }
-        s->ctx.push_back(c);
+        s->lanes.push_back(c);
     }
-    for (int k = 0; k < nslots; ++k) s->workers.emplace_back([s, k] { s->loop(k); });
+    for (int k = 0; k < nl; ++k) s->workers.emplace_back([s, k] { s->loop(k); });
     *out = s;
     return ISPAN_OK;
 }
@@ -236,7 +347,9 @@ int ispan_server_submit(ispan_server *s, const ispan_csr *g, int32_t *labels_out
     if (!s || !g || !ticket) return ISPAN_ERR_ARG;
     if (g->V < 0 || g->E < 0 || (g->V > 0 && !labels_out)) return ISPAN_ERR_ARG;
     if (g->offset_bytes != 4 && g->offset_bytes != 8) return ISPAN_ERR_ARG;
-    if (g->V > s->capV || g->E > s->capE) return ISPAN_ERR_CAPACITY;
+    if (g->V >= INT32_MAX) return ISPAN_ERR_CAPACITY;
+    // a request runs alone if it exceeds the batch limits; it must fit the budget
+    if (lane_region_bytes(g->V, g->E, 1) > s->arena.cap) return ISPAN_ERR_CAPACITY;
     std::lock_guard<std::mutex> lk(s->mu);
     if (s->stop) return ISPAN_ERR_ARG;
     if (s->cfg.max_pending > 0 && (int64_t)s->pending.size() >= s->cfg.max_pending) return ISPAN_ERR_BUSY;
@@ -288,9 +401,12 @@ int ispan_server_wait(ispan_server *s, int64_t ticket, int64_t timeout_us, ispan
 int ispan_server_counters(ispan_server *s, int64_t *out, int32_t n) {
     if (!s || !out) return ISPAN_ERR_ARG;
     std::lock_guard<std::mutex> lk(s->mu);
-    const int64_t v[6] = {s->n_batches, s->n_graphs, s->n_vertices, s->n_edges, s->busy_ns,
-                          (int64_t)s->pending.size()};
-    for (int32_t i = 0; i < n && i < 6; ++i) out[i] = v[i];
+    // busy time includes the batch in flight now
+    const int64_t busy = s->busy_ns + (s->active > 0 ? now_ns() - s->busy_since : 0);
+    const int64_t v[10] = {s->n_batches, s->n_graphs, s->n_vertices, s->n_edges, busy,
+                           (int64_t)s->pending.size(), s->lane_ns, (int64_t)s->arena.used,
+                           (int64_t)s->arena.peak, (int64_t)s->lanes.size()};
+    for (int32_t i = 0; i < n && i < 10; ++i) out[i] = v[i];
     return ISPAN_OK;
 }
 
@@ -303,7 +419,11 @@ int ispan_server_destroy(ispan_server *s) {
     s->cv_work.notify_all();
     for (std::thread &t : s->workers)  // queued requests are served first
         if (t.joinable()) t.join();
-    for (ispan_ctx *c : s->ctx) ispan_ctx_destroy(c);
+    for (ispan_ctx *c : s->lanes) ispan_ctx_destroy(c);
+    if (s->dev_base) {
+        cudaSetDevice(s->device);
+        cudaFree(s->dev_base);
+    }
     delete s;
     return ISPAN_OK;
 }

@@ -14,7 +14,7 @@
 #include "graph.h"
 #include "scc_common.h"
 
-static thread_local int32_t *g_scc_dst = nullptr;
+static thread_local index_t *g_scc_dst = nullptr;
 
 void get_scc_result(index_t *scc_id, index_t vert_count)
 {
@@ -29,16 +29,28 @@ graph *graph_load(const char *a, const char *b, const char *c, const char *d, do
     return new graph(a, b, c, d);
 }
 
+#ifndef ISPAN_REF64
 extern "C" int ispan_ref_run(int32_t V, int32_t E, int32_t *fw_beg, int32_t *fw_adj,
                              int32_t *bw_beg, int32_t *bw_adj, int threads, int alpha,
                              int beta, int gamma, double theta, double *avg_time15,
                              int32_t *scc_id_out, int quiet)
+#else
+// The wide build (oracle/Makefile ref64): the reference compiled with its
+// integer types (src/util.h:17-21) widened to 64 bits, for graphs whose edge
+// count needs 64-bit offsets.
+extern "C" int ispan_ref_run64(int64_t V, int64_t E, int64_t *fw_beg, int64_t *fw_adj,
+                               int64_t *bw_beg, int64_t *bw_adj, int threads, int alpha,
+                               int beta, int gamma, double theta, double *avg_time15,
+                               int64_t *scc_id_out, int quiet)
+#endif
 {
+    static_assert(sizeof(*fw_beg) == sizeof(index_t), "offset width of this build");
+    static_assert(sizeof(*fw_adj) == sizeof(vertex_t), "vertex id width of this build");
     graph g;
-    g.fw_beg_pos = fw_beg;
-    g.fw_csr = fw_adj;
-    g.bw_beg_pos = bw_beg;
-    g.bw_csr = bw_adj;
+    g.fw_beg_pos = (index_t *)fw_beg;
+    g.fw_csr = (vertex_t *)fw_adj;
+    g.bw_beg_pos = (index_t *)bw_beg;
+    g.bw_csr = (vertex_t *)bw_adj;
     g.weight = nullptr;
     g.vert_count = V;
     g.edge_count = E;
@@ -51,9 +63,10 @@ extern "C" int ispan_ref_run(int32_t V, int32_t E, int32_t *fw_beg, int32_t *fw_
         int dn = open("/dev/null", O_WRONLY);
         if (dn >= 0) { dup2(dn, 1); close(dn); }
     }
-    g_scc_dst = scc_id_out;
+    g_scc_dst = (index_t *)scc_id_out;
     scc_detection(&g, alpha, beta, gamma, theta, threads, avg_time15);
     g_scc_dst = nullptr;
-    if (saved >= 0) { fflush(stdout); dup2(saved, 1); close(saved); }
+    fflush(stdout);
+    if (saved >= 0) { dup2(saved, 1); close(saved); }
     return 0;
 }

@@ -114,8 +114,10 @@ def test_server_mix_equals_alone():
 
 
 def test_server_refuses_oversize_request():
-    with Server(max_batch_graphs=4, max_batch_V=1000, max_batch_E=10000, hbm_budget_bytes=1 << 30) as srv:
-        g = G.rmat(12, 8, 1)
+    """A request whose footprint exceeds the whole budget is refused at
+    submission; smaller ones are served."""
+    with Server(max_batch_graphs=4, max_batch_V=1000, max_batch_E=10000, hbm_budget_bytes=16 << 20) as srv:
+        g = G.from_edges(300_000, np.zeros((0, 2), np.int64))  # ~100 B of scratch per vertex > 16 MiB
         out = np.empty(g.V, np.int32)
         with pytest.raises(IspanError) as e:
             srv.submit(g.fw_beg, g.fw_adj, g.bw_beg, g.bw_adj, out)
@@ -125,3 +127,72 @@ def test_server_refuses_oversize_request():
         tk = srv.submit(t.fw_beg, t.fw_adj, t.bw_beg, t.bw_adj, o)
         assert srv.wait(tk, 60)["status"] == 1
         assert np.array_equal(o, oracle.tarjan(t))
+
+
+def _slow_graph():
+    """A 1e6-vertex random DAG of planted cycles (lengths up to 1000): its
+    colouring rounds keep a lane busy for a long time."""
+    import torch
+    from ispan_b200 import gen
+    g = gen.batch(nseg=2, vmin=1_000_000, vmax=1_000_000, ef_min=8, ef_max=8, max_cycle=1000, seed=5)
+    fb, fa, bb, ba = g.extract(1, "int64")  # odd graphs of a batch are the planted DAGs
+    g.free()
+    torch.cuda.synchronize()
+    host = G.CSR(int(fb.numel()) - 1, int(fa.numel()), fb.cpu().numpy(), fa.cpu().numpy(), bb.cpu().numpy(),
+                 ba.cpu().numpy())
+    return (fb, fa, bb, ba), host
+
+
+def test_server_overlaps_requests_that_arrive_mid_batch():
+    """Continuous batching: requests submitted while a long batch is on the
+    GPU are admitted by free lanes and finish before that batch does, and
+    every request's labels are those of its graph run alone (the exact
+    partition)."""
+    import time
+    import torch
+    dev, host = _slow_graph()
+    small = [G.rmat(10, 16, 3), G.planted(3000, 4, giant_frac=0.3), G.toy(), G.random_graph(500, 2000, 1)]
+    with Server(n_slots=4, hbm_budget_bytes=8 << 30) as srv:
+        out_big = torch.full((host.V,), -7, dtype=torch.int32, device="cuda")
+        tb = srv.submit(*dev, out_big)
+        t_wait = time.monotonic() + 60
+        while True:  # until the big request's batch is admitted (it is then on the GPU)
+            info = srv.peek(tb)
+            if info["t_start_ns"] > 0 or time.monotonic() > t_wait:
+                break
+            time.sleep(0.001)
+        assert info["status"] == 0, "the long batch finished before the small requests could be sent"
+        outs, tks = [], []
+        for g in small:
+            o = np.full(max(g.V, 1), -7, np.int32)
+            tks.append(srv.submit(g.fw_beg, g.fw_adj, g.bw_beg, g.bw_adj, o))
+            outs.append(o)
+        small_info = [srv.wait(t, timeout_s=120) for t in tks]
+        still_running = srv.peek(tb)["status"] == 0
+        big = srv.wait(tb, timeout_s=300)
+        assert big["status"] == 1 and all(i["status"] == 1 for i in small_info)
+        assert still_running, "the small requests did not finish while the long batch ran"
+        for i in small_info:
+            assert i["batch_id"] != big["batch_id"] and i["t_done_ns"] < big["t_done_ns"]
+            assert i["t_start_ns"] < big["t_done_ns"]  # admitted while the long batch ran
+        for g, o in zip(small, outs):
+            assert np.array_equal(o[:g.V], oracle.tarjan(g))
+        assert np.array_equal(out_big.cpu().numpy(), oracle.tarjan(host))
+        cnt = srv.counters()
+        assert cnt["bytes_in_use"] == 0 and 0 < cnt["bytes_peak"] <= 8 << 30
+        assert cnt["lane_ns"] > cnt["busy_ns"]  # more than one batch was in flight at times
+
+
+def test_server_single_lane_and_memory_wait():
+    """One lane, and a budget that holds one batch at a time: requests wait
+    for memory, then run; labels are exact."""
+    pool = _mix(5)
+    with Server(n_slots=1, max_batch_graphs=2, hbm_budget_bytes=64 << 20) as srv:
+        outs = [np.full(max(g.V, 1), -7, np.int32) for g in pool]
+        tks = [srv.submit(g.fw_beg, g.fw_adj, g.bw_beg, g.bw_adj, o) for g, o in zip(pool, outs)]
+        infos = [srv.wait(t, timeout_s=120) for t in tks]
+        assert all(i["status"] == 1 for i in infos)
+        for g, o in zip(pool, outs):
+            assert np.array_equal(o[:g.V], oracle.tarjan(g))
+        cnt = srv.counters()
+        assert cnt["lanes"] == 1 and cnt["bytes_peak"] <= 64 << 20 and cnt["bytes_in_use"] == 0

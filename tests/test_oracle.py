@@ -145,3 +145,17 @@ def test_rmat16_restatement_and_reference(path):
         assert np.array_equal(oracle.canon_codes(csr, z[f"ref_codes_t{t}"]), exact)
     labels, _, _ = oracle.ispan(csr)
     assert np.array_equal(labels, exact)
+
+
+@pytest.mark.skipif(not (os.path.exists(oracle.REF_LIB) and
+                         os.path.exists(os.path.join(os.path.dirname(oracle.__file__), "_ref", "libispan_ref64.so"))),
+                    reason="reference builds absent (make -C oracle ref ref64 where the reference tree is)")
+@pytest.mark.parametrize("name,csr", [("rmat14", G.rmat(14, 16, 2)), ("planted3000", G.planted(3000, 2))])
+def test_wide_reference_build_matches_reference(name, csr):
+    """The reference compiled with its 64-bit typedefs (the CPU baseline of
+    graphs beyond int32 offsets) emits the same serial codes as its int32
+    build."""
+    import ref_wide
+    narrow, _ = oracle.ref_run(csr, 1)
+    wide, _ = ref_wide.run(csr.fw_beg, csr.fw_adj, csr.bw_beg, csr.bw_adj, 1)
+    assert np.array_equal(narrow.astype(np.int64), wide)
