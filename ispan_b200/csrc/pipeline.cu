@@ -237,8 +237,10 @@ static int ctx_alloc(ispan_ctx *c) {
 static int ctx_segments(ispan_ctx *c, int64_t nseg) {
     if (nseg <= c->maxSeg) return ISPAN_OK;
     if (c->rg && c->maxSeg > 0) return ISPAN_ERR_CAPACITY;  // a lane's tables were carved for its batch
-    for (void *p : c->seg_owned) cudaFree(p);
-    c->seg_owned.clear();
+    if (!c->rg) {  // a lane frees nothing (cudaFree would synchronise the device); destroy frees these
+        for (void *p : c->seg_owned) cudaFree(p);
+        c->seg_owned.clear();
+    }
     int64_t n = std::max<int64_t>(nseg, 1);
     int rc = 0;
     rc |= dalloc(&c->vbase, n + 1, c->seg_owned, c->rg);
@@ -771,8 +773,10 @@ static int pk_reserve(ispan_ctx *c, int64_t n) {
     if (n <= c->pk_n) return ISPAN_OK;
     if (c->rg && c->pk_n > 0) return ISPAN_ERR_CAPACITY;  // a lane's tables were carved for its batch
     const int64_t m = c->rg ? std::max<int64_t>(n, 1) : std::max<int64_t>({n, 2 * c->pk_n, 64});
-    for (void *q : c->pkt_owned) cudaFree(q);
-    c->pkt_owned.clear();
+    if (!c->rg) {
+        for (void *q : c->pkt_owned) cudaFree(q);
+        c->pkt_owned.clear();
+    }
     c->pk_n = 0;
     int rc = 0;
     rc |= dalloc(&c->pk_desc, m, c->pkt_owned, c->rg);

@@ -73,6 +73,10 @@ def main(argv):
         os.unlink(p)  # the file's memory is freed once widened
     print(f"LOADED {time.time() - t0:.1f} s", flush=True)
     L = _lib()
+    # the pipeline's own printf lines reach the log as they are printed (a
+    # killed run keeps the stages it finished): line-buffered C stdout
+    libc = C.CDLL(None)
+    libc.setvbuf(C.c_void_p.in_dll(libc, "stdout"), None, 1, 0)  # _IOLBF
     t = np.zeros(15, np.float64)
     print("PIPELINE START", flush=True)
     t1 = time.time()
