@@ -325,6 +325,7 @@ static void fill_run(ispan_ctx *c, Run<OffT> &r, Ext<OffT> &x, int64_t V, int64_
     x.large[1] = c->large[1];
     x.cq[0] = c->qv[0];  // the frontier queues are free once the giant is done
     x.cq[1] = c->qv[1];
+    x.cand = c->small;   // free until the WCC stage lists its small components
 }
 
 template <typename Kern, typename... Args>
@@ -367,16 +368,16 @@ static cudaError_t enqueue(ispan_ctx *c, Run<OffT> r, Ext<OffT> x, bool times, b
     LK((k_giant_residual<OffT><<<G, kBlock, 0, s>>>(r, x)));
     if (r.flags & ISPAN_F_EXACT_STATS) LK((k_list_degrees<OffT><<<G, kBlock, 0, s>>>(r, r.wl[0], x.ctl + K_WL0, -1, C_Q1_XDEG)));
     EV(4);
-    if ((e = launch_coop(k_trim1<OffT>, c->g_coop[2], s, r, x, 0, 1))) return e;
+    if ((e = launch_coop(k_trim1<OffT>, c->g_coop[2], s, r, x, 0, 1, 1))) return e;
     if (r.flags & ISPAN_F_EXACT_STATS) LK((k_list_degrees<OffT><<<G, kBlock, 0, s>>>(r, r.wl[1], x.ctl + K_WL1, C_Q2_N, C_Q2_XDEG)));
     EV(5);
-    LK((k_trim2<OffT><<<G, kBlock, 0, s>>>(r, x, 1)));
+    LK((k_trim2<OffT><<<G, kBlock, 0, s>>>(r, x, x.cand, x.ctl + K_CAND)));
     EV(6);
-    LK((k_trim3<OffT><<<G, kBlock, 0, s>>>(r, x, 1)));
+    LK((k_trim3<OffT><<<G, kBlock, 0, s>>>(r, x, x.cand, x.ctl + K_CAND)));
     EV(7);
     if ((e = cudaMemsetAsync(x.ctl + K_CQ0, 0, 3 * sizeof(unsigned long long), s))) return e;
     if ((e = cudaMemsetAsync(x.ctl + K_WL0, 0, sizeof(unsigned long long), s))) return e;
-    if ((e = launch_coop(k_trim1<OffT>, c->g_coop[2], s, r, x, 1, 0))) return e;
+    if ((e = launch_coop(k_trim1<OffT>, c->g_coop[2], s, r, x, 1, 0, 0))) return e;
     EV(8);
     LK((k_wcc_init<OffT><<<G, kBlock, 0, s>>>(r, x, 0)));
     LK((k_wcc_hook<OffT><<<G, kBlock, 0, s>>>(r, x, 0)));

@@ -20,7 +20,7 @@ enum Cls : uint8_t { CLS_NONE = 0, CLS_GIANT = 1, CLS_TRIM1 = 2, CLS_TRIM2 = 3, 
 // control-block slots (Run::ctl64): worklist and queue counters
 enum Ctl64 {
     K_WL0 = 0, K_WL1, K_CQ0, K_CQ1, K_CQ2, K_ROOTS, K_SMALL, K_LARGE, K_ALLOC, K_LARGE2,
-    K_SPILL, K_MICE_SCC, K_LOCAL_NEXT, K_MINPRIO0, K_MINPRIO1, kNumCtl = 32
+    K_SPILL, K_MICE_SCC, K_LOCAL_NEXT, K_MINPRIO0, K_MINPRIO1, K_CAND, kNumCtl = 32
 };
 
 constexpr int kLocalV = 1024;   // a WCC up to this many vertices ...
@@ -33,6 +33,7 @@ struct Ext {
     int32_t *small;               // [V] small WCC roots
     int32_t *large[2];            // [V] vertices of large WCCs (double buffered)
     int32_t *cq[2];               // [V] peel cascade queues
+    int32_t *cand;                // [V] trim-2/3 candidates left by the first peel (count K_CAND)
 };
 
 // ---------------------------------------------------------------------------
@@ -314,7 +315,7 @@ __device__ __forceinline__ void count_active(const OffT *beg, const int32_t *adj
 }
 
 template <typename OffT>
-__global__ void __launch_bounds__(kBlock) k_trim1(Run<OffT> r, Ext<OffT> x, int in, int out) {
+__global__ void __launch_bounds__(kBlock) k_trim1(Run<OffT> r, Ext<OffT> x, int in, int out, int cand) {
     __shared__ int64_t sh[kWarps];
     const int64_t gt = (int64_t)blockIdx.x * kBlock + threadIdx.x;
     const int64_t nt = (int64_t)gridDim.x * kBlock;
@@ -380,10 +381,16 @@ __global__ void __launch_bounds__(kBlock) k_trim1(Run<OffT> r, Ext<OffT> x, int 
         if (!grid_sync(r.gsync, r.err)) return;
         ++lv;
     }
-    // final: peeled vertices leave; survivors move to the other worklist
+    // final: peeled vertices leave; survivors move to the other worklist.
+    // With `cand` set, survivors with at most two active out- or in-edges
+    // (the counters are exact after the cascade) are also listed as the
+    // trim-2/3 candidates: every vertex of a 2- or 3-vertex pattern has at
+    // most two distinct active successors (or predecessors), so without
+    // duplicate edges no pattern is missed; with duplicates a pattern may be
+    // left to the later stages, which find the same SCC.
     int64_t peeled = 0;
     for (int64_t i = gt; i - threadIdx.x < n; i += nt) {
-        bool keep = false;
+        bool keep = false, cd = false;
         int32_t v = 0;
         if (i < n) {
             v = wl[i];
@@ -395,10 +402,12 @@ __global__ void __launch_bounds__(kBlock) k_trim1(Run<OffT> r, Ext<OffT> x, int 
                     ++peeled;
                 } else {
                     keep = true;
+                    cd = cand && (__ldcg(r.cnt_out + v) <= 2 || __ldcg(r.cnt_in + v) <= 2);
                 }
             }
         }
         wl_append(keep, v, r.wl[out], x.ctl + K_WL0 + out);
+        if (cand) wl_append(cd, v, x.cand, x.ctl + K_CAND);
     }
     int64_t tp = block_sum64(peeled, sh);
     if (threadIdx.x == 0) {
@@ -448,10 +457,10 @@ __device__ __forceinline__ bool claim(Run<OffT> &r, Ext<OffT> &x, int32_t v, int
 // active successor has the vertex as its only active successor) and source
 // 2-cycles (the same over predecessors).  Label = min of the pair.
 template <typename OffT>
-__global__ void __launch_bounds__(kBlock) k_trim2(Run<OffT> r, Ext<OffT> x, int in) {
+__global__ void __launch_bounds__(kBlock) k_trim2(Run<OffT> r, Ext<OffT> x, const int32_t *wl,
+                                                  const unsigned long long *n_wl) {
     __shared__ int64_t sh[kWarps];
-    const int64_t n = (int64_t)__ldcg(x.ctl + K_WL0 + in);
-    const int32_t *wl = r.wl[in];
+    const int64_t n = (int64_t)__ldcg(n_wl);
     int64_t got = 0;
     for (int64_t i = (int64_t)blockIdx.x * kBlock + threadIdx.x; i < n; i += (int64_t)gridDim.x * kBlock) {
         int32_t v = wl[i];
@@ -476,10 +485,10 @@ __global__ void __launch_bounds__(kBlock) k_trim2(Run<OffT> r, Ext<OffT> x, int 
 // trim_3_2_from_fq (:881-1080, hub A<->B, A<->C) in one launch: both claim
 // 3-vertex sets, so they may run concurrently.  Label = min of the three.
 template <typename OffT>
-__global__ void __launch_bounds__(kBlock) k_trim3(Run<OffT> r, Ext<OffT> x, int in) {
+__global__ void __launch_bounds__(kBlock) k_trim3(Run<OffT> r, Ext<OffT> x, const int32_t *wl,
+                                                  const unsigned long long *n_wl) {
     __shared__ int64_t sh[kWarps];
-    const int64_t n = (int64_t)__ldcg(x.ctl + K_WL0 + in);
-    const int32_t *wl = r.wl[in];
+    const int64_t n = (int64_t)__ldcg(n_wl);
     int64_t got = 0;
     for (int64_t i = (int64_t)blockIdx.x * kBlock + threadIdx.x; i < n; i += (int64_t)gridDim.x * kBlock) {
         int32_t v = wl[i];
