@@ -254,6 +254,24 @@ int ispan_condense(const ispan_csr *g, const int32_t *labels, uint64_t *pairs_ou
 int ispan_shard_expand(const ispan_csr *rows, int64_t v0, int64_t V, const uint8_t *frontier,
                        const uint8_t *visited, const uint8_t *allowed, uint8_t *next, void *stream);
 
+/* Queue form of a sharded level (what ispan_b200/sharded.py runs).
+ * expand_queue: the owned frontier vertices queue[0 .. *queue_count) (global
+ * ids; the count is read on the device) mark next[w] = 1 (byte per vertex, V
+ * entries) for each neighbour w whose bit is clear in visited[] and, if
+ * allowed is not NULL, set in allowed[] (both bitmaps of V bits, replicated
+ * on every rank).  collect: after the ranks' next maps are merged by a
+ * reduce-scatter (MAX) that leaves this rank its owned slice mine[0 .. n_own)
+ * of the vertices [v0, v0 + n_own) (v0 a multiple of 32), the owned vertices
+ * set there and not yet visited get their visited bit and are appended to
+ * queue (count *queue_count, which the caller zeroes first); the caller then
+ * all-gathers the owned visited words.  Replaces the per-level step of the
+ * reference's MPI variant with its bitmap exchange (src_mpi/fw_bw.h:382-442). */
+int ispan_shard_expand_queue(const ispan_csr *rows, int64_t v0, int64_t V, const int32_t *queue,
+                             const int64_t *queue_count, const uint32_t *visited, const uint32_t *allowed,
+                             uint8_t *next, void *stream);
+int ispan_shard_collect(int64_t v0, int64_t n_own, const uint8_t *mine, uint32_t *visited, int32_t *queue,
+                        int64_t *queue_count, void *stream);
+
 /* Largest graph (vertices) that ispan_scc_small_noalloc accepts. */
 #define ISPAN_NOALLOC_MAX_V 65536
 

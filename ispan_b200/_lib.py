@@ -116,6 +116,8 @@ def lib() -> C.CDLL:
         L.ispan_server_counters.argtypes = [P, P, C.c_int32]
         L.ispan_server_destroy.argtypes = [P]
         L.ispan_shard_expand.argtypes = [C.POINTER(Csr), C.c_int64, C.c_int64, P, P, P, P, P]
+        L.ispan_shard_expand_queue.argtypes = [C.POINTER(Csr), C.c_int64, C.c_int64, P, P, P, P, P, P]
+        L.ispan_shard_collect.argtypes = [C.c_int64, C.c_int64, P, P, P, P, P]
         L.ispan_condense.argtypes = [C.POINTER(Csr), P, P, C.c_int64, C.POINTER(C.c_int64), P]
         L.ispan_ref_codes.argtypes = [P, P]
         L.ispan_debug_trace.argtypes = [P, P, C.c_int64]
@@ -131,7 +133,7 @@ def lib() -> C.CDLL:
 SYMBOLS = ("ispan_ctx_create", "ispan_ctx_destroy", "ispan_ctx_set_stream", "ispan_ctx_bytes", "ispan_scc_run",
            "ispan_scc_run_batch", "ispan_scc_run_graphs", "ispan_graphs_pack", "ispan_graphs_run", "ispan_ctx_set_tuning", "ispan_ctx_get_tuning", "ispan_server_create", "ispan_server_limits",
            "ispan_server_submit", "ispan_server_poll", "ispan_server_wait", "ispan_server_counters",
-           "ispan_server_destroy", "ispan_condense", "ispan_shard_expand", "ispan_ref_codes", "ispan_debug_trace", "ispan_debug_barrier_timeout", "ispan_scc_small_noalloc",
+           "ispan_server_destroy", "ispan_condense", "ispan_shard_expand", "ispan_shard_expand_queue", "ispan_shard_collect", "ispan_ref_codes", "ispan_debug_trace", "ispan_debug_barrier_timeout", "ispan_scc_small_noalloc",
            "ispan_strerror", "ispan_version")
 
 

@@ -13,18 +13,38 @@ import torch.multiprocessing as mp
 
 import oracle
 from ispan_b200 import graphs as G
-from ispan_b200.sharded import giant_scc, reach, split_rows
+from ispan_b200.sharded import bits_to_map, giant_scc, owned_range, reach, split_rows
 
 
-def cpu_expand(rows, V, frontier, visited, allowed, nxt):
-    f = frontier.numpy()
-    vis = visited.numpy()
-    al = None if allowed is None else allowed.numpy()
-    out = nxt.numpy()
-    for i in np.nonzero(f[rows.v0:rows.v0 + rows.n])[0]:
-        for w in rows.adj[rows.beg[i]:rows.beg[i + 1]]:
-            if not vis[w] and (al is None or al[w]):
-                out[w] = 1
+class CpuOps:
+    """CPU stand-ins for the two per-level kernels (ispan_shard_expand_queue,
+    ispan_shard_collect), same contract, on CPU tensors."""
+
+    @staticmethod
+    def expand(rows, V, queue, qn, visited, allowed, nxt):
+        vis = visited.numpy().view(np.uint32)
+        al = None if allowed is None else allowed.numpy().view(np.uint32)
+        out = nxt.numpy()
+        for v in queue.numpy()[:int(qn.item())]:
+            i = int(v) - rows.v0
+            for w in rows.adj[rows.beg[i]:rows.beg[i + 1]]:
+                b = np.uint32(1) << np.uint32(w & 31)
+                if not (vis[w >> 5] & b) and (al is None or (al[w >> 5] & b)):
+                    out[w] = 1
+
+    @staticmethod
+    def collect(v0, n_own, mine, visited, queue, qn):
+        vis = visited.numpy().view(np.uint32)
+        q = queue.numpy()
+        k = int(qn.item())
+        for i in np.nonzero(mine.numpy()[:n_own])[0]:
+            v = v0 + int(i)
+            b = np.uint32(1) << np.uint32(v & 31)
+            if not (vis[v >> 5] & b):
+                vis[v >> 5] |= b
+                q[k] = v
+                k += 1
+        qn.fill_(k)
 
 
 def _port():
@@ -57,7 +77,7 @@ def _worker(rank, world, port, q, kind="planted"):
         p = _pivot(g, exact)
         fw = split_rows(g.fw_beg, g.fw_adj, rank, world)
         bw = split_rows(g.bw_beg, g.bw_adj, rank, world)
-        s = giant_scc(fw, bw, g.V, p, expand=cpu_expand, device="cpu").numpy().astype(bool)
+        s = giant_scc(fw, bw, g.V, p, ops=CpuOps, device="cpu").numpy().astype(bool)
         q.put((rank, bool(np.array_equal(s, exact == exact[p]))))
     except Exception as e:  # noqa: BLE001
         q.put((rank, repr(e)))
@@ -85,7 +105,7 @@ def test_sharded_giant_world_size_2():
 
 
 def test_sharded_giant_world_size_3_uneven_rows():
-    # 2048 vertices over 3 ranks: ranges of 682, 683 and 683 rows
+    # 2048 vertices over 3 ranks: 22, 22 and 20 words of 32 vertices
     res = _run_world(3, "rmat")
     assert res == [(0, True), (1, True), (2, True)], res
 
@@ -94,28 +114,32 @@ def test_split_rows_reassembles_the_csr():
     g = _graph_rmat()
     for world in (1, 2, 3, 5):
         parts = [split_rows(g.fw_beg, g.fw_adj, r, world) for r in range(world)]
-        assert [p.v0 for p in parts] == [g.V * r // world for r in range(world)]
+        assert [p.v0 for p in parts] == [owned_range(g.V, r, world)[0] for r in range(world)]
+        assert all(p.v0 % 32 == 0 for p in parts)  # owned ranges are whole bitmap words
         assert sum(p.n for p in parts) == g.V
         adj = np.concatenate([p.adj for p in parts])
         assert np.array_equal(adj, g.fw_adj)
         deg = np.concatenate([np.diff(p.beg) for p in parts])
         assert np.array_equal(deg, np.diff(g.fw_beg))
-    # more ranks than vertices: empty ranges are valid shards
+    # more ranks than words: empty ranges are valid shards
     tiny_beg, tiny_adj = np.array([0, 1, 2], np.int64), np.array([1, 0], np.int32)
     parts = [split_rows(tiny_beg, tiny_adj, r, 4) for r in range(4)]
-    assert [p.n for p in parts] == [0, 1, 0, 1]
+    assert [p.n for p in parts] == [2, 0, 0, 0]
     assert np.array_equal(np.concatenate([p.adj for p in parts]), tiny_adj)
 
 
-def test_allowed_map_restricts_the_search():
+def test_allowed_bits_restrict_the_search():
     g = _graph()
     exact = oracle.tarjan(g)
     p = _pivot(g, exact)
     fw = split_rows(g.fw_beg, g.fw_adj, 0, 1)
-    full = reach(fw, g.V, [p], None, expand=cpu_expand, device="cpu")
-    allowed = torch.from_numpy((exact == exact[p]).astype(np.uint8))
-    inside = reach(fw, g.V, [p], allowed, expand=cpu_expand, device="cpu")
-    assert int(inside.sum()) == int((exact == exact[p]).sum())  # an SCC is closed under reach inside it
+    full = bits_to_map(reach(fw, g.V, [p], None, ops=CpuOps, device="cpu"), g.V)
+    scc = (exact == exact[p]).astype(np.uint8)
+    words = np.zeros((g.V + 31) // 32, np.uint32)
+    idx = np.nonzero(scc)[0]
+    np.bitwise_or.at(words, idx >> 5, np.uint32(1) << (idx & 31).astype(np.uint32))
+    inside = bits_to_map(reach(fw, g.V, [p], torch.from_numpy(words.view(np.int32)), ops=CpuOps, device="cpu"), g.V)
+    assert int(inside.sum()) == int(scc.sum())  # an SCC is closed under reach inside it
     assert int(full.sum()) >= int(inside.sum())
 
 
@@ -125,5 +149,27 @@ def test_single_rank_matches_oracle():
     p = _pivot(g, exact)
     fw = split_rows(g.fw_beg, g.fw_adj, 0, 1)
     bw = split_rows(g.bw_beg, g.bw_adj, 0, 1)
-    s = giant_scc(fw, bw, g.V, p, expand=cpu_expand, device="cpu").numpy().astype(bool)
+    s = giant_scc(fw, bw, g.V, p, ops=CpuOps, device="cpu").numpy().astype(bool)
     assert np.array_equal(s, exact == exact[p])
+
+
+def test_seed_set_and_empty_graph():
+    g = _graph()
+    exact = oracle.tarjan(g)
+    fw = split_rows(g.fw_beg, g.fw_adj, 0, 1)
+    seeds = [0, 1, 2, 3]
+    got = bits_to_map(reach(fw, g.V, seeds, None, ops=CpuOps, device="cpu"), g.V).numpy().astype(bool)
+    # the union of the seeds' forward sets, by a plain CPU BFS
+    want = np.zeros(g.V, bool)
+    stack = list(seeds)
+    want[seeds] = True
+    while stack:
+        v = stack.pop()
+        for w in g.fw_adj[g.fw_beg[v]:g.fw_beg[v + 1]]:
+            if not want[w]:
+                want[w] = True
+                stack.append(w)
+    assert np.array_equal(got, want)
+    e = split_rows(np.zeros(41, np.int64), np.zeros(0, np.int32), 0, 1)
+    assert int(bits_to_map(reach(e, 40, [7], None, ops=CpuOps, device="cpu"), 40).sum()) == 1
+    del exact
