@@ -171,10 +171,12 @@ struct ispan_ctx {
 static int64_t words_of(int64_t V) { return (V + 31) / 32 + 1; }
 
 static constexpr int kCtlCounters = 0;                       // kNumCounters
-static constexpr int kCtlQpk = kNumCounters;                 // 3
+static constexpr int kCtlQpk = kNumCounters;                 // 3 (forward search)
 static constexpr int kCtlLvl = kNumCounters + 4;             // 12
 static constexpr int kCtlX = kNumCounters + 4 + 16;          // kNumCtl
-static constexpr int kCtlTotal = kCtlX + kNumCtl;
+static constexpr int kCtlQpkB = kCtlX + kNumCtl;             // 3 (backward search: fresh slots,
+static constexpr int kCtlLvlB = kCtlQpkB + 4;                //    no reset between the searches)
+static constexpr int kCtlTotal = kCtlLvlB + 16;
 
 extern "C" int64_t ispan_ctx_bytes(int64_t V, int64_t E) {
     int64_t W = words_of(V);
@@ -346,23 +348,29 @@ static cudaError_t enqueue(ispan_ctx *c, Run<OffT> r, Ext<OffT> x, bool times, b
 #define LK(...) \
     do { __VA_ARGS__; e = cudaGetLastError(); if (e) return e; } while (0)
     EV(0);
-    if ((e = cudaMemsetAsync(ctl, 0, kCtlTotal * sizeof(unsigned long long), s))) return e;
-    if ((e = cudaMemsetAsync(c->hist, 0, (kHistCap + kBigCap) * sizeof(int64_t), s))) return e;
-    if ((e = cudaMemsetAsync(c->gsync, 0, 4 * sizeof(unsigned), s))) return e;
-    if ((e = cudaMemsetAsync(c->err, 0, 4 * sizeof(int), s))) return e;
-    if ((e = cudaMemsetAsync(c->trace, 0, 3 * kTraceLevels * 4 * sizeof(long long), s))) return e;
-    if ((e = cudaMemsetAsync(c->pivot_key, 0, r.nseg * sizeof(unsigned long long), s))) return e;
-    if ((e = cudaMemsetAsync(c->gsize, 0, r.nseg * sizeof(unsigned long long), s))) return e;
-    if ((e = cudaMemsetAsync(c->gmin, 0x7f, r.nseg * sizeof(int32_t), s))) return e;
+    {   // every per-run counter, map and table that starts at zero, in one launch
+        ResetDesc rd;
+        rd.z[0] = {ctl, (int64_t)kCtlTotal * 8};
+        rd.z[1] = {c->hist, (int64_t)(kHistCap + kBigCap) * 8};
+        rd.z[2] = {c->gsync, 4 * 4};
+        rd.z[3] = {c->err, 4 * 4};
+        rd.z[4] = {c->trace, 3 * kTraceLevels * 4 * 8};
+        rd.z[5] = {c->pivot_key, r.nseg * 8};
+        rd.z[6] = {c->gsize, r.nseg * 8};
+        rd.gmin = c->gmin;
+        rd.nseg = r.nseg;
+        LK((k_reset<<<std::min<int64_t>(G, 4 * c->nsm), 256, 0, s>>>(rd)));
+    }
     LK((k_trim1_first<OffT><<<G, kBlock, 0, s>>>(r, x)));
     EV(1);
     LK((k_seed<OffT, 0><<<std::max<int64_t>(1, (r.nseg + 1023) / 1024), 32 * 32, 0, s>>>(r)));
     if ((e = launch_coop(k_bfs<OffT, 0>, c->g_coop[0], s, r, c->bfsctl))) return e;
     EV(2);
-    if ((e = cudaMemsetAsync(r.qpk, 0, 16 * sizeof(unsigned long long) + 4 * 8, s))) return e;
-    if ((e = cudaMemsetAsync(r.lvl, 0, 16 * sizeof(unsigned long long), s))) return e;
-    LK((k_seed<OffT, 1><<<std::max<int64_t>(1, (r.nseg + 1023) / 1024), 32 * 32, 0, s>>>(r)));
-    if ((e = launch_coop(k_bfs<OffT, 1>, c->g_coop[1], s, r, c->bfsctl))) return e;
+    Run<OffT> rb = r;  // the backward search counts in its own queue and level slots
+    rb.qpk = ctl + kCtlQpkB;
+    rb.lvl = ctl + kCtlLvlB;
+    LK((k_seed<OffT, 1><<<std::max<int64_t>(1, (r.nseg + 1023) / 1024), 32 * 32, 0, s>>>(rb)));
+    if ((e = launch_coop(k_bfs<OffT, 1>, c->g_coop[1], s, rb, c->bfsctl))) return e;
     if (r.flags & ISPAN_F_EXACT_STATS) LK((k_reach_degrees<OffT><<<G, kBlock, 0, s>>>(r)));
     EV(3);
     LK((k_giant_residual<OffT><<<G, kBlock, 0, s>>>(r, x)));
@@ -375,8 +383,7 @@ static cudaError_t enqueue(ispan_ctx *c, Run<OffT> r, Ext<OffT> x, bool times, b
     EV(6);
     LK((k_trim3<OffT><<<G, kBlock, 0, s>>>(r, x, x.cand, x.ctl + K_CAND)));
     EV(7);
-    if ((e = cudaMemsetAsync(x.ctl + K_CQ0, 0, 3 * sizeof(unsigned long long), s))) return e;
-    if ((e = cudaMemsetAsync(x.ctl + K_WL0, 0, sizeof(unsigned long long), s))) return e;
+    // the first peel left its cascade counters and the consumed list count at zero
     if ((e = launch_coop(k_trim1<OffT>, c->g_coop[2], s, r, x, 1, 0, 0))) return e;
     EV(8);
     LK((k_wcc_init<OffT><<<G, kBlock, 0, s>>>(r, x, 0)));

@@ -74,6 +74,28 @@ __device__ void compact_words(int64_t W, WordFn f, int32_t *out, unsigned long l
 }
 
 // ---------------------------------------------------------------------------
+// Per-run reset: zero the run's counters, histogram, barrier and error
+// words, trace and per-graph tables, and set the per-graph giant minima to
+// "none", in one launch (each range a multiple of 4 bytes).
+struct ResetRange { void *p; int64_t bytes; };
+struct ResetDesc {
+    ResetRange z[7];
+    int32_t *gmin;
+    int64_t nseg;
+};
+
+__global__ void k_reset(ResetDesc d) {
+    const int64_t gt = (int64_t)blockIdx.x * blockDim.x + threadIdx.x, nt = (int64_t)gridDim.x * blockDim.x;
+#pragma unroll 1
+    for (int k = 0; k < 7; ++k) {
+        uint32_t *p = reinterpret_cast<uint32_t *>(d.z[k].p);
+        const int64_t n = d.z[k].bytes / 4;
+        for (int64_t i = gt; i < n; i += nt) p[i] = 0u;
+    }
+    for (int64_t i = gt; i < d.nseg; i += nt) d.gmin[i] = 0x7f7f7f7f;
+}
+
+// ---------------------------------------------------------------------------
 // Input check on the device: offsets monotone from 0 to E, every adjacency
 // id in [0, V).  The reference's loader trusts its files (src/graph.cpp:2-92);
 // here a malformed CSR is reported as ISPAN_ERR_ARG before any stage reads it.
@@ -344,12 +366,20 @@ __global__ void __launch_bounds__(kBlock) k_trim1(Run<OffT> r, Ext<OffT> x, int 
         wl_append(dead, v, x.cq[0], cqc + 0);
     }
     if (!grid_sync(r.gsync, r.err)) return;
+    // every CTA has read the list count: with `cand` (the first peel) it is
+    // cleared for the second peel, which appends its survivors there
+    if (cand && blockIdx.x == 0 && threadIdx.x == 0) x.ctl[K_WL0 + in] = 0ull;
     // cascade rounds
     int lv = 0;
     for (int guard = 0; guard < (1 << 30); ++guard) {
         const int c = lv & 1;
         const int64_t m = (int64_t)__ldcg(cqc + lv % 3);
-        if (m == 0) break;
+        if (m == 0) {
+            // every CTA reads this zero slot; the other two are free, and the
+            // second peel starts its cascade from three zero counters
+            if (cand && blockIdx.x == 0 && threadIdx.x == 0) { cqc[(lv + 1) % 3] = 0ull; cqc[(lv + 2) % 3] = 0ull; }
+            break;
+        }
         if (blockIdx.x == 0 && threadIdx.x == 0) cqc[(lv + 2) % 3] = 0ull;
         const int32_t *q = x.cq[c];
         for (int64_t i = gt; i - threadIdx.x < m; i += nt) {
