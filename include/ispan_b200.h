@@ -122,6 +122,9 @@ typedef struct {
     int32_t color_levels;     /* colouring large WCCs: a warp works up to 4 * color_levels chunks of 32
                                  frontier entries per grid round before handing the rest back (32) */
     int32_t color_pivots;     /* about this many pivots in the first colouring round; doubles per round (1024) */
+    int32_t color_compact;    /* colour the large WCCs on a compact copy of their subgraph (dense ids,
+                                 only their edges among themselves): 1 on, -1 off (0: default, on) */
+    int32_t reserved;
 } ispan_tuning;
 
 /* NULL restores the defaults; the next run re-captures its CUDA graph. */

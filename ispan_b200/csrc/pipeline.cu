@@ -25,8 +25,9 @@
 
 #include "bfs.cuh"
 #include "pack.cuh"
-#include "stages.cuh"
+#include "compact.cuh"
 #include "lane.h"
+#include "stages.cuh"
 
 using namespace ispan;
 
@@ -145,11 +146,11 @@ struct ispan_ctx {
     unsigned long long *h_counters = nullptr;  // pinned
     int *h_err = nullptr;
 
-    ispan_tuning tuning = {0, 0, 0, 0, 0, 0};
+    ispan_tuning tuning = {0, 0, 0, 0, 0, 0, 0, 0};
 
     // launch geometry
     int g_stream = 0;           // grid for plain grid-stride kernels
-    int g_coop[4] = {0, 0, 0, 0};  // bfs<0>, bfs<1>, trim1, color (per offset width)
+    int g_coop[5] = {0, 0, 0, 0, 0};  // bfs<0>, bfs<1>, trim1, color, color on the compact graph
     int g_coop_w = 0;           // offset width the coop grids were computed for
 
     // CUDA graph cache
@@ -330,6 +331,68 @@ static void fill_run(ispan_ctx *c, Run<OffT> &r, Ext<OffT> &x, int64_t V, int64_
     x.cand = c->small;   // free until the WCC stage lists its small components
 }
 
+// The run descriptor of the colouring on the compact graph: the same state
+// arrays, the compact CSR (int32 offsets) and the compact-to-original map.
+template <typename OffT>
+static void compact_run(const Run<OffT> &r, const Ext<OffT> &x, const CmpBufs &b, Run<int32_t> &rc,
+                        Ext<int32_t> &xc) {
+    memset(&rc, 0, sizeof rc);
+    memset(&xc, 0, sizeof xc);
+    rc.V = r.V;  // an upper bound: the compact vertex count is read on the device
+    rc.E = r.E;
+    rc.W = r.W;
+    rc.nseg = r.nseg;
+    rc.vbase = r.vbase;
+    rc.fw_beg = b.fbeg;
+    rc.bw_beg = b.bbeg;
+    rc.fw_adj = b.fadj;
+    rc.bw_adj = b.badj;
+    rc.label = r.label;
+    rc.A = r.A; rc.F = r.F; rc.B = r.B; rc.D = r.D; rc.P = r.P; rc.T = r.T;
+    for (int i = 0; i < 2; ++i) {
+        rc.qv[i] = r.qv[i];
+        rc.qe[i] = r.qe[i];
+        rc.qchunk[i] = r.qchunk[i];
+        rc.wl[i] = r.wl[i];
+    }
+    rc.qpk = r.qpk;
+    rc.lvl = r.lvl;
+    rc.wlc = r.wlc;
+    rc.cnt_out = r.cnt_out;
+    rc.cnt_in = r.cnt_in;
+    rc.parent = r.parent;
+    rc.aux = r.aux;
+    rc.aux2 = r.aux2;
+    rc.members = r.members;
+    rc.pivot_key = r.pivot_key;
+    rc.gmin = r.gmin;
+    rc.gsize = r.gsize;
+    rc.cls = r.cls;
+    rc.counters = r.counters;
+    rc.hist = r.hist;
+    rc.gsync = r.gsync;
+    rc.trace = r.trace;
+    rc.err = r.err;
+    rc.alpha = r.alpha;
+    rc.beta = r.beta;
+    rc.gamma = r.gamma;
+    rc.flags = r.flags;
+    rc.async_v = r.async_v;
+    rc.async_e = r.async_e;
+    rc.async_deg = r.async_deg;
+    rc.color_levels = r.color_levels;
+    rc.color_pivots = r.color_pivots;
+    xc.ctl = x.ctl;
+    xc.roots = x.roots;
+    xc.small = x.small;
+    xc.large[0] = x.large[0];
+    xc.large[1] = x.large[1];
+    xc.cq[0] = x.cq[0];
+    xc.cq[1] = x.cq[1];
+    xc.cand = x.cand;
+    xc.old = b.old;
+}
+
 template <typename Kern, typename... Args>
 static cudaError_t launch_coop(Kern k, int grid, cudaStream_t s, Args... args) {
     void *ptrs[] = {(void *)&args...};
@@ -394,6 +457,31 @@ static cudaError_t enqueue(ispan_ctx *c, Run<OffT> r, Ext<OffT> x, bool times, b
     EV(9);
     LK((k_local_scc<OffT><<<c->nsm * 6, kLocalThreads, 0, s>>>(r, x)));
     EV(10);
+    if (c->tuning.color_compact >= 0) {
+        // the large WCCs' subgraph in dense ids (compact.cuh), then the
+        // colouring on it; the input-graph form returns at once if it was built
+        CmpBufs b;
+        b.newid = c->cnt_out;
+        b.old = c->small;
+        b.dout = c->members;
+        b.din = c->roots;
+        b.fbeg = reinterpret_cast<int32_t *>(c->qe[1]);
+        b.bbeg = b.fbeg + (r.V + 1);
+        b.fadj = c->wl[0];
+        b.badj = c->wl[1];
+        b.bsum = reinterpret_cast<long long *>(c->aux);
+        b.cap_e = r.V;
+        const int nblk = (int)std::max<int64_t>(1, std::min<int64_t>(kScanBlocks, r.V / 4));
+        LK((k_cmp_ids<OffT><<<G, kBlock, 0, s>>>(r, x, b)));
+        LK((k_cmp_count<OffT><<<nblk, kBlock, 0, s>>>(r, x, b)));
+        LK((k_cmp_tops<<<1, 32, 0, s>>>(x.ctl, b, nblk)));
+        LK((k_cmp_offsets<OffT><<<nblk, kBlock, 0, s>>>(r, x, b)));
+        LK((k_cmp_fill<OffT><<<G, kBlock, 0, s>>>(r, x, b)));
+        Run<int32_t> rc;
+        Ext<int32_t> xc;
+        compact_run(r, x, b, rc, xc);
+        if ((e = launch_coop(k_color<int32_t>, c->g_coop[4], s, rc, xc))) return e;
+    }
     if ((e = launch_coop(k_color<OffT>, c->g_coop[3], s, r, x))) return e;
     EV(11);
     LK((k_finalize<OffT><<<G, kBlock, 0, s>>>(r, x)));
@@ -418,7 +506,8 @@ static int coop_setup(ispan_ctx *c) {
         for (int i = 0; i < 2; ++i) c->g_coop[i] = std::min(c->g_coop[i], want * nsm);
     c->g_coop[2] = coop_grid(k_trim1<OffT>, nsm, kBlock);
     c->g_coop[3] = coop_grid(k_color<OffT>, nsm, kBlock);
-    for (int i = 0; i < 4; ++i)
+    c->g_coop[4] = coop_grid(k_color<int32_t>, nsm, kBlock);
+    for (int i = 0; i < 5; ++i)
         if (c->g_coop[i] < 1) return ISPAN_ERR_CUDA;
     c->g_coop_w = w;
     return ISPAN_OK;
@@ -1100,7 +1189,7 @@ int ispan_ctx_set_tuning(ispan_ctx *c, const ispan_tuning *t) {
               t->color_pivots < 0))
         return ISPAN_ERR_ARG;
     std::lock_guard<std::mutex> lock(c->mu);
-    c->tuning = t ? *t : ispan_tuning{0, 0, 0, 0, 0, 0};
+    c->tuning = t ? *t : ispan_tuning{0, 0, 0, 0, 0, 0, 0, 0};
     c->g_coop_w = 0;  // recompute the persistent grids
     if (c->gexec) {   // the captured graph holds the old values
         cudaGraphExecDestroy(c->gexec);
@@ -1118,6 +1207,8 @@ int ispan_ctx_get_tuning(ispan_ctx *c, ispan_tuning *t) {
     t->bfs_ctas_per_sm = c->tuning.bfs_ctas_per_sm;
     t->color_levels = c->tuning.color_levels > 0 ? c->tuning.color_levels : kCLevels;
     t->color_pivots = c->tuning.color_pivots > 0 ? c->tuning.color_pivots : kCPivots;
+    t->color_compact = c->tuning.color_compact >= 0 ? 1 : -1;
+    t->reserved = 0;
     return ISPAN_OK;
 }
 

@@ -20,7 +20,9 @@ enum Cls : uint8_t { CLS_NONE = 0, CLS_GIANT = 1, CLS_TRIM1 = 2, CLS_TRIM2 = 3, 
 // control-block slots (Run::ctl64): worklist and queue counters
 enum Ctl64 {
     K_WL0 = 0, K_WL1, K_CQ0, K_CQ1, K_CQ2, K_ROOTS, K_SMALL, K_LARGE, K_ALLOC, K_LARGE2,
-    K_SPILL, K_MICE_SCC, K_LOCAL_NEXT, K_MINPRIO0, K_MINPRIO1, K_CAND, kNumCtl = 32
+    K_SPILL, K_MICE_SCC, K_LOCAL_NEXT, K_MINPRIO0, K_MINPRIO1, K_CAND,
+    K_CMP_OK, K_CMP_EF, K_CMP_EB,  // compact colouring graph: built (1), its edge counts
+    kNumCtl = 32
 };
 
 constexpr int kLocalV = 1024;   // a WCC up to this many vertices ...
@@ -34,7 +36,15 @@ struct Ext {
     int32_t *large[2];            // [V] vertices of large WCCs (double buffered)
     int32_t *cq[2];               // [V] peel cascade queues
     int32_t *cand;                // [V] trim-2/3 candidates left by the first peel (count K_CAND)
+    const int32_t *old;           // colouring on the compact graph: original id of each compact id
+                                  // (NULL: the colouring runs on the input graph's ids)
 };
+
+// original vertex id of a colouring vertex id
+template <typename OffT>
+__device__ __forceinline__ int32_t orig_id(const Ext<OffT> &x, int32_t v) {
+    return x.old ? __ldg(x.old + v) : v;
+}
 
 // ---------------------------------------------------------------------------
 // Block-level compaction of bitmap words into a worklist with one atomic per
@@ -1256,10 +1266,14 @@ __device__ __forceinline__ int color_async(const Run<OffT> &r, const Ext<OffT> &
     return -1;
 }
 
+// Runs on the input graph's ids (x.old NULL) unless the compact graph was
+// built, or on the compact graph (x.old set, r holding its CSR) if it was;
+// the pipeline launches both forms and one of them returns at once.
 template <typename OffT>
 __global__ void __launch_bounds__(kBlock, 2) k_color(Run<OffT> r, Ext<OffT> x) {
     __shared__ int64_t sh[kWarps];
     __shared__ ColorSmem sm;
+    if ((__ldcg(x.ctl + K_CMP_OK) != 0) != (x.old != nullptr)) return;
     const int64_t gt = (int64_t)blockIdx.x * kBlock + threadIdx.x;
     const int64_t nt = (int64_t)gridDim.x * kBlock;
     // class (high half) and colour (low half) of each vertex in one word
@@ -1277,13 +1291,16 @@ __global__ void __launch_bounds__(kBlock, 2) k_color(Run<OffT> r, Ext<OffT> x) {
         while (shift0 < 30 && (n >> (shift0 + 1)) >= r.color_pivots) ++shift0;
         if (blockIdx.x == 0 && threadIdx.x == 0) x.ctl[K_MINPRIO0] = ~0ull;
         if (n == 0) return;
-        // every word dead first: neighbours outside the large WCCs fail the class compare
-        for (int64_t i = gt; i < r.V; i += nt) cc[i] = kDeadWord;
+        // every word dead first: neighbours outside the large WCCs fail the class
+        // compare (the compact graph has no such neighbours; its ids are < n)
+        const int64_t nw = x.old ? n : r.V;
+        for (int64_t i = gt; i < nw; i += nt) cc[i] = kDeadWord;
         if (!grid_sync(r.gsync, r.err)) return;
         uint32_t pm = 0xffffffffu;
         for (int64_t i = gt; i < n; i += nt) {
             int32_t v = x.large[0][i];
-            cc[v] = ((unsigned long long)(uint32_t)r.parent[v] << 32) | ((unsigned long long)kNoColour << 1) | 1ull;
+            cc[v] = ((unsigned long long)(uint32_t)r.parent[orig_id(x, v)] << 32) |
+                    ((unsigned long long)kNoColour << 1) | 1ull;
             pm = min(pm, prio_of((uint32_t)v));
         }
         pm = __reduce_min_sync(0xffffffffu, pm);
@@ -1344,7 +1361,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_color(Run<OffT> r, Ext<OffT> x) {
                 if (rt) {
                     set_bit(r.F, v);
                     rootof[v] = v;
-                    mn[v] = v;
+                    mn[v] = orig_id(x, v);
                     szc[v] = 0;
                 }
             }
@@ -1366,7 +1383,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_color(Run<OffT> r, Ext<OffT> x) {
             int32_t v = L[i];
             if (bitv(r.F, v)) {
                 const int32_t rv = __ldcg(rootof + v);
-                atomicMin(mn + rv, v);
+                atomicMin(mn + rv, orig_id(x, v));  // labels are original ids
                 atomicAdd(szc + rv, 1);
             }
         }
@@ -1380,9 +1397,10 @@ __global__ void __launch_bounds__(kBlock, 2) k_color(Run<OffT> r, Ext<OffT> x) {
                 v = L[i];
                 if (bitv(r.F, v)) {
                     const int32_t rv = __ldcg(rootof + v);
-                    r.label[v] = __ldcg(mn + rv);
-                    r.cls[v] = CLS_MICE;
-                    clear_bit(r.A, v);
+                    const int32_t ov = orig_id(x, v);
+                    r.label[ov] = __ldcg(mn + rv);
+                    r.cls[ov] = CLS_MICE;
+                    clear_bit(r.A, ov);
                     cc[v] = kDeadWord;
                     ++nl;
                     if (rv == v) {  // one histogram entry per SCC, at its root
