@@ -196,9 +196,9 @@ typedef struct {
                                    creation); 0: 64 GiB */
     int64_t max_batch_V;        /* vertices / edges of a batch of several graphs; 0:
                                    the largest */
-    int64_t max_batch_E;        /*   at 16 edges per vertex in budget / n_slots.  A
-                                   single larger request runs alone if its footprint
-                                   fits the budget */
+    int64_t max_batch_E;        /*   at 16 edges per vertex in half the budget (the whole
+                                   budget with one lane).  A single larger request runs
+                                   alone if its footprint fits the budget */
     int64_t max_wait_us;        /* a partial batch waits this long for more requests */
     int64_t max_pending;        /* queued requests before submit returns ISPAN_ERR_BUSY; 0: no limit */
     ispan_params params;

@@ -273,7 +273,10 @@ int ispan_server_create(const ispan_server_config *cfg, ispan_server **out) {
     // each lane's L2 window would evict the others' maps; lanes run without
     s->params.flags = (s->params.flags | ISPAN_F_NO_L2_WINDOW) & ~(uint32_t)ISPAN_F_LABELS_ON_DEVICE;
     s->capN = cfg->max_batch_graphs > 0 ? cfg->max_batch_graphs : 4096;
-    const int64_t share = budget / nl;  // per-batch size limit: a lane's share of the budget
+    // per-batch size limit: half the budget whatever the lane count (a batch's
+    // time is set mostly by its slowest graph, so fuller batches serve more
+    // requests per unit of time; two such batches still fit side by side)
+    const int64_t share = nl == 1 ? budget : budget / 2;
     if (cfg->max_batch_V > 0 && cfg->max_batch_E >= 0) {
         s->capV = cfg->max_batch_V;
         s->capE = cfg->max_batch_E;
