@@ -9,7 +9,7 @@
 //   trim-1 peel (fixpoint)    k_trim1                  (persistent, cooperative)
 //   trim-2, trim-3            k_trim2, k_trim3
 //   trim-1 peel again         k_trim1
-//   WCC                       k_wcc_init/hook/flatten/alloc/scatter
+//   WCC                       k_wcc_init/hook/compress/giant/hook/flatten/alloc/scatter
 //   mice: small WCCs          k_local_scc              (shared-memory Tarjan)
 //   mice: large WCCs          k_color                  (persistent, cooperative)
 //   canonical labels          k_finalize
@@ -450,7 +450,10 @@ static cudaError_t enqueue(ispan_ctx *c, Run<OffT> r, Ext<OffT> x, bool times, b
     if ((e = launch_coop(k_trim1<OffT>, c->g_coop[2], s, r, x, 1, 0, 0))) return e;
     EV(8);
     LK((k_wcc_init<OffT><<<G, kBlock, 0, s>>>(r, x, 0)));
-    LK((k_wcc_hook<OffT><<<G, kBlock, 0, s>>>(r, x, 0)));
+    LK((k_wcc_hook<OffT><<<G, kBlock, 0, s>>>(r, x, 0, 0)));
+    LK((k_wcc_compress<OffT><<<G, kBlock, 0, s>>>(r, x, 0)));
+    LK((k_wcc_giant<OffT><<<1, kWccRootSamples, 0, s>>>(r, x, 0)));
+    LK((k_wcc_hook<OffT><<<G, kBlock, 0, s>>>(r, x, 0, 1)));
     LK((k_wcc_flatten<OffT><<<G, kBlock, 0, s>>>(r, x, 0)));
     LK((k_wcc_alloc<OffT><<<G, kBlock, 0, s>>>(r, x)));
     LK((k_wcc_scatter<OffT><<<G, kBlock, 0, s>>>(r, x, 0)));

@@ -22,6 +22,7 @@ enum Ctl64 {
     K_WL0 = 0, K_WL1, K_CQ0, K_CQ1, K_CQ2, K_ROOTS, K_SMALL, K_LARGE, K_ALLOC, K_LARGE2,
     K_SPILL, K_MICE_SCC, K_LOCAL_NEXT, K_MINPRIO0, K_MINPRIO1, K_CAND,
     K_CMP_OK, K_CMP_EF, K_CMP_EB,  // compact colouring graph: built (1), its edge counts
+    K_WCC_GIANT,                   // (root << 32) | 1 when one WCC holds half the root sample
     kNumCtl = 32
 };
 
@@ -339,9 +340,13 @@ __device__ __forceinline__ void count_active(const OffT *beg, const int32_t *adj
                                              int32_t &n) {
     int64_t e0 = ld_off(beg, v), e1 = ld_off(beg, v + 1);
     int c = 0;
-    for (int64_t e = e0; e < e1; ++e) {
-        int32_t w = ld_adj(adj, e);
-        c += (w != v) && bitc(A, w);
+    // four ids, then their active bits, each group of loads in flight together
+    for (int64_t e = e0; e < e1; e += 4) {
+        int32_t w[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) w[q] = e + q < e1 ? ld_adj(adj, e + q) : (int32_t)v;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) c += (w[q] != v) && bitc(A, w[q]);
     }
     n = c;
 }
@@ -364,7 +369,7 @@ __global__ void __launch_bounds__(kBlock) k_trim1(Run<OffT> r, Ext<OffT> x, int 
             if (bitc(r.A, v)) {
                 int32_t o, ii;
                 count_active(r.fw_beg, r.fw_adj, r.A, v, o);
-                count_active(r.bw_beg, r.bw_adj, r.A, v, ii);
+                count_active(r.bw_beg, r.bw_adj, r.A, v, ii);  // independent of o: both in flight
                 if (o == 0 || ii == 0) {
                     dead = set_bit(r.D, v);
                 } else {
@@ -603,36 +608,98 @@ __global__ void __launch_bounds__(kBlock) k_wcc_init(Run<OffT> r, Ext<OffT> x, i
     }
 }
 
-template <typename OffT>
-__global__ void __launch_bounds__(kBlock) k_wcc_hook(Run<OffT> r, Ext<OffT> x, int in) {
-    const int64_t n = (int64_t)__ldcg(x.ctl + K_WL0 + in);
-    for (int64_t i = (int64_t)blockIdx.x * kBlock + threadIdx.x; i < n; i += (int64_t)gridDim.x * kBlock) {
-        int32_t v = r.wl[in][i];
-        int64_t e0 = ld_off(r.fw_beg, v), e1 = ld_off(r.fw_beg, v + 1);
-        for (int64_t e = e0; e < e1; e += 4) {
-            // four neighbours' ids, then their active bits, in flight together
-            int32_t ws[4];
+// hook the active neighbours adj[e0, e1) of v (four ids, then their active
+// bits, in flight together)
+__device__ __forceinline__ void hook_range(int32_t *parent, const uint32_t *A, const int32_t *adj, int32_t v,
+                                           int64_t e0, int64_t e1) {
+    for (int64_t e = e0; e < e1; e += 4) {
+        int32_t ws[4];
 #pragma unroll
-            for (int q = 0; q < 4; ++q) ws[q] = e + q < e1 ? ld_adj(r.fw_adj, e + q) : v;
-            bool act[4];
+        for (int q = 0; q < 4; ++q) ws[q] = e + q < e1 ? ld_adj(adj, e + q) : v;
+        bool act[4];
 #pragma unroll
-            for (int q = 0; q < 4; ++q) act[q] = ws[q] != v && bitc(r.A, ws[q]);
+        for (int q = 0; q < 4; ++q) act[q] = ws[q] != v && bitc(A, ws[q]);
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                if (!act[q]) continue;
-                int32_t a = v, b = ws[q];
-                for (int guard = 0; guard < (1 << 20); ++guard) {
-                    a = uf_find(r.parent, a);
-                    b = uf_find(r.parent, b);
-                    if (a == b) break;
-                    if (a > b) { int32_t t = a; a = b; b = t; }
-                    int32_t old = atomicCAS(r.parent + b, b, a);  // hook root b under a
-                    if (old == b) break;
-                    b = old;
-                }
+        for (int q = 0; q < 4; ++q) {
+            if (!act[q]) continue;
+            int32_t a = v, b = ws[q];
+            for (int guard = 0; guard < (1 << 20); ++guard) {
+                a = uf_find(parent, a);
+                b = uf_find(parent, b);
+                if (a == b) break;
+                if (a > b) { int32_t t = a; a = b; b = t; }
+                int32_t old = atomicCAS(parent + b, b, a);  // hook root b under a
+                if (old == b) break;
+                b = old;
             }
         }
     }
+}
+
+// Hooking in the manner of Afforest (neighbour sampling): phase 0 links
+// every vertex with its first kWccSample out-neighbours; after a compress
+// pass and a sample of the roots, phase 1 links the rest.  When one
+// component holds at least half of the sample (a giant WCC), its members
+// skip phase 1: every edge with an endpoint outside it is linked from that
+// endpoint (its remaining out-edges and all its in-edges), and edges inside
+// it are already connected.  Otherwise every vertex links its remaining
+// out-edges.
+constexpr int kWccSample = 2;
+constexpr int kWccRootSamples = 1024;
+
+template <typename OffT>
+__global__ void __launch_bounds__(kBlock) k_wcc_hook(Run<OffT> r, Ext<OffT> x, int in, int phase) {
+    const int64_t n = (int64_t)__ldcg(x.ctl + K_WL0 + in);
+    const bool skip_giant = phase == 1 && __ldcg(x.ctl + K_WCC_GIANT) != 0;
+    const int32_t g = (int32_t)(__ldcg(x.ctl + K_WCC_GIANT) >> 32);
+    for (int64_t i = (int64_t)blockIdx.x * kBlock + threadIdx.x; i < n; i += (int64_t)gridDim.x * kBlock) {
+        int32_t v = r.wl[in][i];
+        const int64_t e0 = ld_off(r.fw_beg, v), e1 = ld_off(r.fw_beg, v + 1);
+        const int64_t es = min(e1, e0 + kWccSample);
+        if (phase == 0) {
+            hook_range(r.parent, r.A, r.fw_adj, v, e0, es);
+        } else if (!skip_giant) {
+            hook_range(r.parent, r.A, r.fw_adj, v, es, e1);
+        } else if (__ldcg(r.parent + v) != g) {
+            hook_range(r.parent, r.A, r.fw_adj, v, es, e1);
+            hook_range(r.parent, r.A, r.bw_adj, v, ld_off(r.bw_beg, v), ld_off(r.bw_beg, v + 1));
+        }
+    }
+}
+
+// after phase 0: every vertex points at its root (read-only walks; no hook
+// runs concurrently), then one CTA samples the roots of evenly spaced
+// vertices and records the most frequent one if it holds half the sample
+template <typename OffT>
+__global__ void __launch_bounds__(kBlock) k_wcc_compress(Run<OffT> r, Ext<OffT> x, int in) {
+    const int64_t n = (int64_t)__ldcg(x.ctl + K_WL0 + in);
+    for (int64_t i = (int64_t)blockIdx.x * kBlock + threadIdx.x; i < n; i += (int64_t)gridDim.x * kBlock) {
+        const int32_t v = r.wl[in][i];
+        r.parent[v] = uf_root(r.parent, v);
+    }
+}
+
+template <typename OffT>
+__global__ void __launch_bounds__(kWccRootSamples) k_wcc_giant(Run<OffT> r, Ext<OffT> x, int in) {
+    __shared__ int32_t roots[kWccRootSamples];
+    __shared__ int best, best_n;
+    const int64_t n = (int64_t)__ldcg(x.ctl + K_WL0 + in);
+    const int t = threadIdx.x;
+    const int ns = (int)(n < kWccRootSamples ? n : kWccRootSamples);
+    if (t < ns) roots[t] = __ldcg(r.parent + r.wl[in][(int64_t)t * n / ns]);
+    if (t == 0) { best = -1; best_n = 0; }
+    __syncthreads();
+    int cnt = 0;
+    if (t < ns) {
+        const int32_t me = roots[t];
+        for (int k = 0; k < ns; ++k) cnt += roots[k] == me;
+        atomicMax(&best_n, cnt);
+    }
+    __syncthreads();
+    if (t < ns && cnt == best_n) atomicMax(&best, roots[t]);  // one root among the most frequent
+    __syncthreads();
+    if (t == 0)
+        x.ctl[K_WCC_GIANT] = (ns > 0 && 2 * best_n >= ns) ? (((unsigned long long)(uint32_t)best << 32) | 1ull) : 0ull;
 }
 
 // flatten, count members per root, list the roots
