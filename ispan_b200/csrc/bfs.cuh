@@ -245,9 +245,19 @@ __device__ __forceinline__ bool bu_pull(const BfsDir<OffT, DIR> &d, int64_t v, i
         rm &= rm - 1;
         int64_t le = __shfl_sync(kFull, e, l), lend = __shfl_sync(kFull, end, l);
         bool hit = false;
-        for (int64_t b = le; b < lend; b += 32) {
-            int64_t i = b + lane;
-            bool h = i < lend && bitv(d.Vm, ld_adj(d.padj, i));
+        // 128 edges per step: four ids per lane, then their four visit bits,
+        // each group of loads in flight together (a hub's list costs a
+        // quarter of the dependent round trips of 32-edge steps)
+        for (int64_t b = le; b < lend; b += 128) {
+            int32_t u[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int64_t i = b + q * 32 + lane;
+                u[q] = i < lend ? ld_adj(d.padj, i) : -1;
+            }
+            bool h = false;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) h |= u[q] >= 0 && bitv(d.Vm, u[q]);
             if (__any_sync(kFull, h)) { hit = true; break; }
         }
         if (lane == l) found = hit;
