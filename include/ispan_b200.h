@@ -194,11 +194,11 @@ typedef struct {
     int32_t reserved;
     int64_t hbm_budget_bytes;   /* device memory the server holds (allocated at
                                    creation); 0: 64 GiB */
-    int64_t max_batch_V;        /* vertices / edges of a batch of several graphs; 0:
-                                   the largest */
-    int64_t max_batch_E;        /*   at 16 edges per vertex in half the budget (the whole
-                                   budget with one lane).  A single larger request runs
-                                   alone if its footprint fits the budget */
+    int64_t max_batch_V;        /* vertices / edges of a batch of several graphs (0: no */
+    int64_t max_batch_E;        /*   limit but the footprint one).  A batch of several
+                                   graphs takes at most half the budget (the whole budget
+                                   with one lane); a single larger request runs alone if its
+                                   footprint fits the budget */
     int64_t max_wait_us;        /* a partial batch waits this long for more requests */
     int64_t max_pending;        /* queued requests before submit returns ISPAN_ERR_BUSY; 0: no limit */
     ispan_params params;

@@ -26,7 +26,9 @@
 
 namespace ispan {
 
-constexpr int kScanBlocks = 1024;  // blocks of the offset scans
+constexpr int kScanBlocks = 1024;  // blocks of the offset scans (at most; one CTA scans their sums)
+constexpr int64_t kCmpMin = 1 << 16;  // fewer colouring vertices than this: no compact graph (the
+                                      // input graph's colour words of so few vertices stay in L2)
 
 struct CmpBufs {
     int32_t *newid;   // [V]
@@ -42,6 +44,7 @@ struct CmpBufs {
 template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_cmp_ids(Run<OffT> r, Ext<OffT> x, CmpBufs b) {
     const int64_t n = (int64_t)__ldcg(x.ctl + K_LARGE);
+    if (n < kCmpMin) return;
     for (int64_t i = (int64_t)blockIdx.x * kBlock + threadIdx.x; i < n; i += (int64_t)gridDim.x * kBlock) {
         const int32_t v = x.large[0][i];
         b.newid[v] = (int32_t)i;
@@ -54,6 +57,7 @@ template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_cmp_count(Run<OffT> r, Ext<OffT> x, CmpBufs b) {
     __shared__ int64_t sh[kWarps];
     const int64_t n = (int64_t)__ldcg(x.ctl + K_LARGE);
+    if (n < kCmpMin) return;
     const int64_t per = (n + gridDim.x - 1) / gridDim.x;
     const int64_t i0 = min(n, (int64_t)blockIdx.x * per), i1 = min(n, i0 + per);
     int64_t so = 0, si = 0;
@@ -80,22 +84,52 @@ __global__ void __launch_bounds__(kBlock) k_cmp_count(Run<OffT> r, Ext<OffT> x, 
     }
 }
 
-// one CTA: exclusive scan of the block sums; the graph is built only if
-// both directions fit
-__global__ void k_cmp_tops(unsigned long long *ctl, CmpBufs b, int nblk) {
-    if (threadIdx.x != 0) return;
-    long long o = 0, in = 0;
-    for (int k = 0; k < nblk; ++k) {
-        const long long a = b.bsum[k], c = b.bsum[kScanBlocks + k];
-        b.bsum[k] = o;
-        b.bsum[kScanBlocks + k] = in;
-        o += a;
-        in += c;
+// one CTA of kScanBlocks threads: exclusive scan of the block sums (a
+// thread per block sum, warp scans, then the warp totals); the graph is
+// built only if both directions fit
+__global__ void __launch_bounds__(kScanBlocks) k_cmp_tops(unsigned long long *ctl, CmpBufs b, int nblk) {
+    __shared__ long long wt[2][kScanBlocks / 32];
+    const int64_t n = (int64_t)__ldcg(ctl + K_LARGE);
+    if (n < kCmpMin) {
+        if (threadIdx.x == 0) ctl[K_CMP_OK] = 0ull;
+        return;
     }
-    const bool fits = o <= b.cap_e && in <= b.cap_e && o < INT32_MAX && in < INT32_MAX && ctl[K_LARGE] > 0;
-    ctl[K_CMP_EF] = (unsigned long long)o;
-    ctl[K_CMP_EB] = (unsigned long long)in;
-    ctl[K_CMP_OK] = fits ? 1ull : 0ull;
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    long long v[2], incl[2];
+    for (int d = 0; d < 2; ++d) {
+        v[d] = t < nblk ? b.bsum[d * kScanBlocks + t] : 0;
+        incl[d] = v[d];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const long long y = __shfl_up_sync(kFull, incl[d], o);
+            if (lane >= o) incl[d] += y;
+        }
+        if (lane == 31) wt[d][warp] = incl[d];
+    }
+    __syncthreads();
+    if (warp == 0) {
+        for (int d = 0; d < 2; ++d) {
+            long long x = wt[d][lane], xi = x;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const long long y = __shfl_up_sync(kFull, xi, o);
+                if (lane >= o) xi += y;
+            }
+            wt[d][lane] = xi - x;  // exclusive base of each warp
+            if (lane == 31) {
+                if (d == 0) ctl[K_CMP_EF] = (unsigned long long)xi;
+                else ctl[K_CMP_EB] = (unsigned long long)xi;
+            }
+        }
+    }
+    __syncthreads();
+    for (int d = 0; d < 2; ++d)
+        if (t < nblk) b.bsum[d * kScanBlocks + t] = wt[d][warp] + incl[d] - v[d];
+    if (t == 0) {
+        const long long o = (long long)ctl[K_CMP_EF], in = (long long)ctl[K_CMP_EB];
+        const bool fits = o <= b.cap_e && in <= b.cap_e && o < INT32_MAX && in < INT32_MAX;
+        ctl[K_CMP_OK] = fits ? 1ull : 0ull;
+    }
 }
 
 // offsets: each block rescans its range from its base (serial per thread

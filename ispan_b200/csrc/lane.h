@@ -14,11 +14,13 @@
 #include "../../include/ispan_b200.h"
 
 // device bytes a lane needs for a batch of n graphs with V vertices and E
-// edges in total: every scratch array, the union CSR and its tables
-size_t lane_region_bytes(int64_t V, int64_t E, int64_t n);
+// edges in total, V_host of the vertices in host-resident graphs (whose
+// offsets are staged on the device): every scratch array, the union CSR and
+// its tables
+size_t lane_region_bytes(int64_t V, int64_t E, int64_t n, int64_t V_host);
 // carve the batch's arrays out of [base, base + bytes); the lane is then
 // ready for ispan_graphs_pack / ispan_graphs_run of that batch
-int lane_bind(ispan_ctx *c, void *base, size_t bytes, int64_t V, int64_t E, int64_t n);
+int lane_bind(ispan_ctx *c, void *base, size_t bytes, int64_t V, int64_t E, int64_t n, int64_t V_host);
 // the region is handed back (the caller frees it in its budget)
 void lane_unbind(ispan_ctx *c);
 // persistent grids sized for nsm SMs

@@ -109,7 +109,8 @@ struct ispan_ctx {
     // union buffers of ispan_scc_run_graphs (allocated on first use)
     int64_t *pk_fwb = nullptr, *pk_bwb = nullptr;  // [maxV + 1]
     int32_t *pk_fwa = nullptr, *pk_bwa = nullptr;  // [maxE]
-    int64_t *pk_stage = nullptr;                   // staged host offsets [2 * (maxV + pk_n)]
+    int64_t *pk_stage = nullptr;                   // staged host offsets [2 * (stage_V + pk_n)]
+    int64_t stage_V = -1;                          // vertices of host graphs a batch may stage (-1: maxV)
     PackDesc *pk_desc = nullptr;                   // [pk_n]
     int64_t *pk_vb = nullptr, *pk_eb = nullptr;    // [pk_n + 1]
     PackDesc *h_desc = nullptr;                    // pinned mirrors
@@ -477,7 +478,7 @@ static cudaError_t enqueue(ispan_ctx *c, Run<OffT> r, Ext<OffT> x, bool times, b
         const int nblk = (int)std::max<int64_t>(1, std::min<int64_t>(kScanBlocks, r.V / 4));
         LK((k_cmp_ids<OffT><<<G, kBlock, 0, s>>>(r, x, b)));
         LK((k_cmp_count<OffT><<<nblk, kBlock, 0, s>>>(r, x, b)));
-        LK((k_cmp_tops<<<1, 32, 0, s>>>(x.ctl, b, nblk)));
+        LK((k_cmp_tops<<<1, kScanBlocks, 0, s>>>(x.ctl, b, nblk)));
         LK((k_cmp_offsets<OffT><<<nblk, kBlock, 0, s>>>(r, x, b)));
         LK((k_cmp_fill<OffT><<<G, kBlock, 0, s>>>(r, x, b)));
         Run<int32_t> rc;
@@ -881,7 +882,7 @@ static int pk_reserve(ispan_ctx *c, int64_t n) {
     int rc = 0;
     rc |= dalloc(&c->pk_desc, m, c->pkt_owned, c->rg);
     rc |= dalloc(&c->pk_vb, 2 * (m + 1), c->pkt_owned, c->rg);
-    rc |= dalloc(&c->pk_stage, 2 * (c->maxV + m), c->pkt_owned, c->rg);
+    rc |= dalloc(&c->pk_stage, 2 * ((c->stage_V >= 0 ? c->stage_V : c->maxV) + m), c->pkt_owned, c->rg);
     if (rc) return ISPAN_ERR_NOMEM;
     c->pk_eb = c->pk_vb + (m + 1);
     c->pk_n = m;
@@ -1027,9 +1028,10 @@ static int run_graphs(ispan_ctx *c, const ispan_csr *gs, int32_t n, int32_t *con
 
 // Carve every scratch array for a batch of n graphs with V vertices and E
 // edges in total; with a null base the region only measures.
-static int ctx_carve(ispan_ctx *c, int64_t V, int64_t E, int64_t n) {
+static int ctx_carve(ispan_ctx *c, int64_t V, int64_t E, int64_t n, int64_t V_host) {
     c->maxV = V;
     c->maxE = E;
+    c->stage_V = V_host;  // only host graphs' offsets are staged
     c->maxSeg = 0;
     c->pk_fwb = c->pk_bwb = nullptr;
     c->pk_fwa = c->pk_bwa = nullptr;
@@ -1041,17 +1043,17 @@ static int ctx_carve(ispan_ctx *c, int64_t V, int64_t E, int64_t n) {
     return rc;
 }
 
-size_t lane_region_bytes(int64_t V, int64_t E, int64_t n) {
+size_t lane_region_bytes(int64_t V, int64_t E, int64_t n, int64_t V_host) {
     ispan_ctx m;
     Region r;  // null base: measure only
     m.rg = &r;
     m.h_cap = INT64_MAX;  // no pinned mirrors for a measurement
-    ctx_carve(&m, V, E, n);
+    ctx_carve(&m, V, E, n, V_host);
     m.rg = nullptr;
     return r.used + 256;
 }
 
-int lane_bind(ispan_ctx *c, void *base, size_t bytes, int64_t V, int64_t E, int64_t n) {
+int lane_bind(ispan_ctx *c, void *base, size_t bytes, int64_t V, int64_t E, int64_t n, int64_t V_host) {
     std::lock_guard<std::mutex> lock(c->mu);
     if (cudaSetDevice(c->device) != cudaSuccess) return ISPAN_ERR_CUDA;
     Region &r = c->lane_region;
@@ -1065,7 +1067,7 @@ int lane_bind(ispan_ctx *c, void *base, size_t bytes, int64_t V, int64_t E, int6
     }
     c->vbase_host.clear();
     c->g_coop_w = 0;
-    const int rc = ctx_carve(c, V, E, n);
+    const int rc = ctx_carve(c, V, E, n, V_host);
     if (rc) {
         c->rg = nullptr;
         c->maxV = c->maxE = 0;
@@ -1076,6 +1078,7 @@ int lane_bind(ispan_ctx *c, void *base, size_t bytes, int64_t V, int64_t E, int6
 void lane_unbind(ispan_ctx *c) {
     std::lock_guard<std::mutex> lock(c->mu);
     c->rg = nullptr;
+    c->stage_V = -1;
     c->maxV = c->maxE = c->maxSeg = 0;  // nothing runs on a lane between batches
     c->pk_fwb = c->pk_bwb = nullptr;
     c->pk_fwa = c->pk_bwa = nullptr;

@@ -114,6 +114,7 @@ struct ispan_server {
     std::vector<ispan_ctx *> lanes;
     int64_t capV = 0, capE = 0;     // per-batch limits when a batch holds more than one graph
     int32_t capN = 0;
+    size_t cap_bytes = 0;           // per-batch footprint limit (several graphs)
     char *dev_base = nullptr;       // the budget
     Arena arena;
     std::mutex mu;
@@ -133,12 +134,13 @@ struct ispan_server {
 
     // pack and run one batch on lane c inside its region
     int pack_run(ispan_ctx *c, char *base, size_t bytes, std::vector<ispan_csr> &gs, std::vector<int32_t *> &labs) {
-        int64_t V = 0, E = 0;
+        int64_t V = 0, E = 0, Vh = 0;
         for (const ispan_csr &g : gs) {
             V += g.V;
             E += g.E;
+            Vh += g.on_device ? 0 : g.V;
         }
-        int rc = lane_bind(c, base, bytes, V, E, (int64_t)gs.size());
+        int rc = lane_bind(c, base, bytes, V, E, (int64_t)gs.size(), Vh);
         if (!rc) rc = ispan_graphs_pack(c, gs.data(), (int32_t)gs.size());
         if (!rc) rc = ispan_graphs_run(c, gs.data(), (int32_t)gs.size(), labs.data(), &params, nullptr);
         lane_unbind(c);
@@ -150,21 +152,27 @@ struct ispan_server {
     // false when nothing can be admitted now
     bool admit(std::vector<int64_t> &take, size_t *off, size_t *bytes) {
         const int64_t share = ((int64_t)pending.size() + idle - 1) / std::max(1, idle);
-        int64_t v = 0, e = 0;
+        int64_t v = 0, e = 0, vh = 0;
         for (int64_t t : pending) {
             if ((int64_t)take.size() >= std::min<int64_t>(capN, std::max<int64_t>(share, 1))) break;
             const Req &r = reqs.at(t);
-            if (!take.empty() && (v + r.g.V > capV || e + r.g.E > capE)) break;
+            const int64_t rh = r.g.on_device ? 0 : r.g.V;
+            if (!take.empty() &&
+                (v + r.g.V > capV || e + r.g.E > capE ||
+                 lane_region_bytes(v + r.g.V, e + r.g.E, (int64_t)take.size() + 1, vh + rh) > cap_bytes))
+                break;
             v += r.g.V;
             e += r.g.E;
+            vh += rh;
             take.push_back(t);
         }
         while (!take.empty()) {
-            *bytes = lane_region_bytes(v, e, (int64_t)take.size());
+            *bytes = lane_region_bytes(v, e, (int64_t)take.size(), vh);
             if (arena.alloc(*bytes, off)) return true;
             const Req &r = reqs.at(take.back());
             v -= r.g.V;
             e -= r.g.E;
+            vh -= r.g.on_device ? 0 : r.g.V;
             take.pop_back();
         }
         return false;
@@ -273,30 +281,26 @@ int ispan_server_create(const ispan_server_config *cfg, ispan_server **out) {
     // each lane's L2 window would evict the others' maps; lanes run without
     s->params.flags = (s->params.flags | ISPAN_F_NO_L2_WINDOW) & ~(uint32_t)ISPAN_F_LABELS_ON_DEVICE;
     s->capN = cfg->max_batch_graphs > 0 ? cfg->max_batch_graphs : 4096;
-    // per-batch size limit: half the budget whatever the lane count (a batch's
-    // time is set mostly by its slowest graph, so fuller batches serve more
-    // requests per unit of time; two such batches still fit side by side)
+    // per-batch size limit: a footprint of half the budget whatever the lane
+    // count (a batch's time is set mostly by its slowest graph, so fuller
+    // batches serve more requests per unit of time; two such batches still fit
+    // side by side), the whole budget with one lane
     const int64_t share = nl == 1 ? budget : budget / 2;
+    s->cap_bytes = (size_t)share;
     if (cfg->max_batch_V > 0 && cfg->max_batch_E >= 0) {
         s->capV = cfg->max_batch_V;
         s->capE = cfg->max_batch_E;
-        if ((int64_t)lane_region_bytes(s->capV, s->capE, s->capN) > budget) {
+        if ((int64_t)lane_region_bytes(s->capV, s->capE, s->capN, s->capV) > budget) {
             delete s;
             return ISPAN_ERR_NOMEM;
         }
     } else {
-        // the largest batch at 16 edges per vertex within a lane's share
-        int64_t lo = 0, hi = (int64_t)INT32_MAX - 64;
-        while (lo < hi) {
-            int64_t mid = (lo + hi + 1) / 2;
-            if ((int64_t)lane_region_bytes(mid, 16 * mid, s->capN) <= share) lo = mid; else hi = mid - 1;
-        }
-        if (lo < 1024) {
+        s->capV = INT32_MAX - 64;  // the footprint limit decides
+        s->capE = INT64_MAX / 4;
+        if ((int64_t)lane_region_bytes(1024, 16 * 1024, 1, 1024) > share) {
             delete s;
             return ISPAN_ERR_NOMEM;
         }
-        s->capV = lo;
-        s->capE = 16 * lo;
     }
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
@@ -352,7 +356,7 @@ int ispan_server_submit(ispan_server *s, const ispan_csr *g, int32_t *labels_out
     if (g->offset_bytes != 4 && g->offset_bytes != 8) return ISPAN_ERR_ARG;
     if (g->V >= INT32_MAX) return ISPAN_ERR_CAPACITY;
     // a request runs alone if it exceeds the batch limits; it must fit the budget
-    if (lane_region_bytes(g->V, g->E, 1) > s->arena.cap) return ISPAN_ERR_CAPACITY;
+    if (lane_region_bytes(g->V, g->E, 1, g->on_device ? 0 : g->V) > s->arena.cap) return ISPAN_ERR_CAPACITY;
     std::lock_guard<std::mutex> lk(s->mu);
     if (s->stop) return ISPAN_ERR_ARG;
     if (s->cfg.max_pending > 0 && (int64_t)s->pending.size() >= s->cfg.max_pending) return ISPAN_ERR_BUSY;

@@ -149,3 +149,19 @@ def test_rmat16_against_reference_fixture(ctx, path):
     labels, _ = ctx.run_csr(csr)
     assert np.array_equal(labels, ref)
     assert st["giant_size"] == int((z["ref_codes_t16"][:csr.V] == 1).sum())
+
+
+@pytest.mark.parametrize("compact", [1, -1])
+def test_colouring_on_compact_graph_and_input_graph(compact):
+    """More than 65,536 vertices reach the colouring (a DAG of planted cycles
+    with no giant SCC), so the compact colouring graph is built when it is on;
+    both forms give the exact partition."""
+    g = G.planted(150000, 12, giant_frac=0.0, dag_ef=3.0, max_cycle=400)
+    with Context(g.V, g.E) as c:
+        c.set_tuning(color_compact=compact)
+        labels, st = c.run_csr(g, histogram=True)
+        assert st["color_rounds"] > 0
+        exact = oracle.tarjan(g)
+        assert np.array_equal(labels, exact)
+        assert st["histogram"] == oracle.histogram(exact)
+        assert c.tuning()["color_compact"] == compact
