@@ -14,13 +14,15 @@
 //   original id -> compact id   r.cnt_out    (int32, valid where A is set)
 //   out/in degrees              r.members, x.roots
 //   offsets (int32)             r.qe[1] viewed as int32: out at [0, n], in at [V+1, V+1+n]
-//   adjacency (int32)           r.wl[0] (out), r.wl[1] (in)
+//   adjacency (int32)           r.wl[0..1] (out), r.members..x.roots (in, written once the
+//                               degrees there are scanned); each pair is one block of 2 V
 // so the random accesses of the rounds fall on n colour words instead of V,
 // and no edge check lands on a vertex outside.  The graph is built only when
 // each direction's edges fit the adjacency arrays (at most V entries, int32
 // offsets); otherwise K_CMP_OK stays 0 and the colouring runs on the input
 // graph.  Membership is the active map A: at this point exactly the vertices
-// of the large WCCs are active.
+// of the large WCCs are active.  The fill kernel reads only the offsets, so
+// the in-adjacency may overwrite the degree arrays.
 #pragma once
 #include "stages.cuh"
 
@@ -35,7 +37,7 @@ struct CmpBufs {
     int32_t *old;     // [n]
     int32_t *dout, *din;
     int32_t *fbeg, *bbeg;  // [n + 1] each
-    int32_t *fadj, *badj;  // [V] each (capacity)
+    int32_t *fadj, *badj;  // [cap_e] each
     long long *bsum;       // [2 * kScanBlocks]
     int64_t cap_e;         // adjacency capacity per direction
 };

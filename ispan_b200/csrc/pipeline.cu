@@ -126,6 +126,7 @@ struct ispan_ctx {
     int64_t *qe[2] = {nullptr, nullptr};
     int32_t *qchunk[2] = {nullptr, nullptr};
     int32_t *wl[2] = {nullptr, nullptr};
+    int32_t *wl4 = nullptr;  // wl[0], wl[1], members, roots: one block of 4 x (maxV + 32)
     int32_t *cnt_out = nullptr, *cnt_in = nullptr, *parent = nullptr, *aux = nullptr, *aux2 = nullptr,
             *members = nullptr, *roots = nullptr, *small = nullptr, *large[2] = {nullptr, nullptr};
     unsigned long long *ctlblk = nullptr;  // counters | qpk | lvl | ctl64
@@ -218,7 +219,7 @@ static int ctx_alloc(ispan_ctx *c) {
         rc |= dalloc(&c->qv[i], V, o, g);
         rc |= dalloc(&c->qe[i], V + 1, o, g);
         rc |= dalloc(&c->qchunk[i], E / kChunk + 4, o, g);
-        rc |= dalloc(&c->wl[i], V, o, g);
+
         rc |= dalloc(&c->large[i], V, o, g);
     }
     rc |= dalloc(&c->cnt_out, V, o, g);
@@ -226,8 +227,16 @@ static int ctx_alloc(ispan_ctx *c) {
     rc |= dalloc(&c->parent, V, o, g);
     rc |= dalloc(&c->aux, V, o, g);
     rc |= dalloc(&c->aux2, V, o, g);
-    rc |= dalloc(&c->members, V, o, g);
-    rc |= dalloc(&c->roots, V, o, g);
+    // the two worklists, then the WCC member and root lists, in one block:
+    // the compact colouring graph (compact.cuh) uses the first two as one
+    // out-adjacency array of 2 V entries and the last two as the in-adjacency
+    rc |= dalloc(&c->wl4, 4 * V, o, g);
+    if (!rc) {
+        c->wl[0] = c->wl4;
+        c->wl[1] = c->wl4 + V;
+        c->members = c->wl4 + 2 * V;
+        c->roots = c->wl4 + 3 * V;
+    }
     rc |= dalloc(&c->small, V, o, g);
     rc |= dalloc(&c->ctlblk, kCtlTotal, o, g);
     rc |= dalloc(&c->hist, kHistCap + kBigCap, o, g);
@@ -471,10 +480,12 @@ static cudaError_t enqueue(ispan_ctx *c, Run<OffT> r, Ext<OffT> x, bool times, b
         b.din = c->roots;
         b.fbeg = reinterpret_cast<int32_t *>(c->qe[1]);
         b.bbeg = b.fbeg + (r.V + 1);
+        // adjacency: out-edges over wl[0..1], in-edges over members/roots (free
+        // once the degrees they hold are scanned), 2 (maxV + 32) entries each
         b.fadj = c->wl[0];
-        b.badj = c->wl[1];
+        b.badj = c->members;
         b.bsum = reinterpret_cast<long long *>(c->aux);
-        b.cap_e = r.V;
+        b.cap_e = 2 * (c->maxV + 32);
         const int nblk = (int)std::max<int64_t>(1, std::min<int64_t>(kScanBlocks, r.V / 4));
         LK((k_cmp_ids<OffT><<<G, kBlock, 0, s>>>(r, x, b)));
         LK((k_cmp_count<OffT><<<nblk, kBlock, 0, s>>>(r, x, b)));
