@@ -59,6 +59,7 @@ def load_table(path: str = TABLE) -> dict:
         with open(path) as f:
             return json.load(f)
     return {"classes": {}}
+    return {"classes": {}}
 
 
 def lookup(V: int, E: int, nseg: int = 1, path: str = TABLE) -> dict | None:

@@ -42,19 +42,8 @@ struct CmpBufs {
     int64_t cap_e;         // adjacency capacity per direction
 };
 
-// ids: compact id i <-> original id L[i]
-template <typename OffT>
-__global__ void __launch_bounds__(kBlock) k_cmp_ids(Run<OffT> r, Ext<OffT> x, CmpBufs b) {
-    const int64_t n = (int64_t)__ldcg(x.ctl + K_LARGE);
-    if (n < kCmpMin) return;
-    for (int64_t i = (int64_t)blockIdx.x * kBlock + threadIdx.x; i < n; i += (int64_t)gridDim.x * kBlock) {
-        const int32_t v = x.large[0][i];
-        b.newid[v] = (int32_t)i;
-        b.old[i] = v;
-    }
-}
-
-// active out- and in-degrees (self-loops dropped), and per scan block sums
+// ids (compact id i <-> original id L[i]), active out- and in-degrees
+// (self-loops dropped), and the per scan block sums of the degrees
 template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_cmp_count(Run<OffT> r, Ext<OffT> x, CmpBufs b) {
     __shared__ int64_t sh[kWarps];
@@ -64,7 +53,9 @@ __global__ void __launch_bounds__(kBlock) k_cmp_count(Run<OffT> r, Ext<OffT> x, 
     const int64_t i0 = min(n, (int64_t)blockIdx.x * per), i1 = min(n, i0 + per);
     int64_t so = 0, si = 0;
     for (int64_t i = i0 + threadIdx.x; i < i1; i += kBlock) {
-        const int32_t v = b.old[i];
+        const int32_t v = x.large[0][i];
+        b.newid[v] = (int32_t)i;
+        b.old[i] = v;
         int32_t co = 0, ci = 0;
         for (int64_t e = ld_off(r.fw_beg, v), e1 = ld_off(r.fw_beg, v + 1); e < e1; ++e) {
             const int32_t w = ld_adj(r.fw_adj, e);

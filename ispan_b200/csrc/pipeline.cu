@@ -470,7 +470,7 @@ static cudaError_t enqueue(ispan_ctx *c, Run<OffT> r, Ext<OffT> x, bool times, b
     EV(9);
     LK((k_local_scc<OffT><<<c->nsm * 6, kLocalThreads, 0, s>>>(r, x)));
     EV(10);
-    if (c->tuning.color_compact >= 0) {
+    if (c->tuning.color_compact >= 0 && r.V > kCmpMin) {  // (smaller graphs never reach kCmpMin)
         // the large WCCs' subgraph in dense ids (compact.cuh), then the
         // colouring on it; the input-graph form returns at once if it was built
         CmpBufs b;
@@ -487,7 +487,6 @@ static cudaError_t enqueue(ispan_ctx *c, Run<OffT> r, Ext<OffT> x, bool times, b
         b.bsum = reinterpret_cast<long long *>(c->aux);
         b.cap_e = 2 * (c->maxV + 32);
         const int nblk = (int)std::max<int64_t>(1, std::min<int64_t>(kScanBlocks, r.V / 4));
-        LK((k_cmp_ids<OffT><<<G, kBlock, 0, s>>>(r, x, b)));
         LK((k_cmp_count<OffT><<<nblk, kBlock, 0, s>>>(r, x, b)));
         LK((k_cmp_tops<<<1, kScanBlocks, 0, s>>>(x.ctl, b, nblk)));
         LK((k_cmp_offsets<OffT><<<nblk, kBlock, 0, s>>>(r, x, b)));
