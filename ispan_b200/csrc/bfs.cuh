@@ -324,6 +324,10 @@ __device__ __forceinline__ void bu_words(const Run<OffT> &r, const BfsDir<OffT, 
                 msum_other += pdeg;
             }
         }
+        // more groups than warps: the next one comes from the level counter
+        // (on small graphs every warp's own group is the only one, and 10^3
+        // warps' atomics on one counter would cost more than the level)
+        if ((r.W + gsz - 1) / gsz <= nwarps) break;
         unsigned long long nx = 0;
         if (lane == 0) nx = atomicAdd(next_group, 1ull);
         g = nwarps + (int64_t)__shfl_sync(kFull, nx, 0);

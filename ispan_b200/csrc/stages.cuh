@@ -645,7 +645,8 @@ __device__ __forceinline__ void hook_range(int32_t *parent, const uint32_t *A, c
 // it are already connected.  Otherwise every vertex links its remaining
 // out-edges.
 constexpr int kWccSample = 2;
-constexpr int kWccRootSamples = 1024;
+constexpr int kWccRootSamples = 512;
+constexpr int64_t kWccSkipMin = 1 << 14;  // smaller worklists: no sample, everyone links everything
 
 template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_wcc_hook(Run<OffT> r, Ext<OffT> x, int in, int phase) {
@@ -685,6 +686,9 @@ __global__ void __launch_bounds__(kWccRootSamples) k_wcc_giant(Run<OffT> r, Ext<
     __shared__ int best, best_n;
     const int64_t n = (int64_t)__ldcg(x.ctl + K_WL0 + in);
     const int t = threadIdx.x;
+    if (n < kWccSkipMin) {  // (the reset left K_WCC_GIANT at zero)
+        return;
+    }
     const int ns = (int)(n < kWccRootSamples ? n : kWccRootSamples);
     if (t < ns) roots[t] = __ldcg(r.parent + r.wl[in][(int64_t)t * n / ns]);
     if (t == 0) { best = -1; best_n = 0; }
