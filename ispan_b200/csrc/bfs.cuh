@@ -11,7 +11,11 @@
 //   TD   top-down over a frontier queue.  The queue is an edge prefix built by
 //        the producers (see q_append), so work is split into equal chunks of
 //        kChunk edges regardless of the degree skew: a hub's adjacency is
-//        spread over many CTAs, a run of low-degree vertices shares one chunk.
+//        spread over many CTAs, a run of low-degree vertices shares one chunk
+//        (this edge-balanced split replaces binning vertices by degree into
+//        thread/warp/CTA expansion).  Each thread reads four consecutive
+//        adjacency entries, as one int4 load when they are 16-byte aligned in
+//        one list.
 //   BU   bottom-up pull over the 1-bit maps, one warp per 32-vertex word.
 //        Each unvisited candidate scans its reverse edges and stops at the
 //        first visited neighbour of any level (the reference's "Rsync" rule),
@@ -156,13 +160,29 @@ __device__ __forceinline__ void td_chunk(const Run<OffT> &r, const BfsDir<OffT, 
             if (sm.qe[mid] <= my0) lo = mid; else hi = mid - 1;
         }
         int i = lo;
+        // the thread's four virtual edges in one adjacency list at a 16-byte
+        // aligned address: one vectorised int4 load; otherwise (a list
+        // boundary inside the group, the chunk's end, a misaligned address)
+        // one load per edge
+        const int64_t p0 = sm.base[i] + my0;
+        const bool one_list = my0 + kPer <= e1 && (i + 1 >= ns || sm.qe[i + 1] >= my0 + kPer);
+#ifdef ISPAN_CHECKED
+        const bool vec = false;  // the checked build range-checks every id
+#else
+        const bool vec = kPer == 4 && one_list && ((uintptr_t)(d.xadj + p0) & 15) == 0;
+#endif
+        if (vec) {
+            const int4 q = __ldg(reinterpret_cast<const int4 *>(d.xadj + p0));
+            w[0] = q.x; w[1] = q.y; w[2] = q.z; w[3] = q.w;
+        } else {
 #pragma unroll
-        for (int k = 0; k < kPer; ++k) {
-            int64_t e = my0 + k;
-            w[k] = -1;
-            if (e < e1) {
-                while (i + 1 < ns && sm.qe[i + 1] <= e) ++i;
-                w[k] = ld_adj(d.xadj, sm.base[i] + e);
+            for (int k = 0; k < kPer; ++k) {
+                int64_t e = my0 + k;
+                w[k] = -1;
+                if (e < e1) {
+                    while (i + 1 < ns && sm.qe[i + 1] <= e) ++i;
+                    w[k] = ld_adj(d.xadj, sm.base[i] + e);
+                }
             }
         }
     } else {
