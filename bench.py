@@ -403,7 +403,7 @@ def bench_social(args, ws, rank, local):
     ctx.set_stream(stream)
     fb, fa, bb, ba = g.ptrs  # the generator's device arrays, no copy
     labels = torch.empty(g.V, dtype=torch.int32, device="cuda")
-    tp = autotune.apply(ctx, g.V, g.E)  # the tuned launch parameters of this graph's shape class
+    tp = autotune.apply(ctx, g.V, g.E, overrides=args.tuning)  # the tuned launch parameters of this graph's shape class
     tun = dict(alpha=tp["alpha"], beta=tp["beta"], gamma=tp["gamma"])
     run = lambda: ctx.run_raw(g.V, g.E, fb, fa, bb, ba, 8, labels, stage_times=True, **tun)  # noqa: E731
     ms_per_step, step_ms, stages, clk = timed_runs(run, stream, args.steps, args.warmup, ws)
@@ -467,6 +467,8 @@ def bench_rmat16(args):
     stream = torch.cuda.Stream()
     ctx = Context(1 << 16, 1 << 21)
     ctx.set_stream(stream)
+    if args.tuning:
+        ctx.set_tuning(**{k: int(v) for k, v in args.tuning.items()})
     per, cpu_ms, e2e_ms, st_last = [], [], [], None
     mism_oracle = mism_ref = n_fixtures = 0
     roofs = []
@@ -475,9 +477,13 @@ def bench_rmat16(args):
         csr = G.rmat(16, 16, seed)
         d = [torch.from_numpy(a).cuda() for a in (csr.fw_beg, csr.fw_adj, csr.bw_beg, csr.bw_adj)]
         lab = torch.empty(csr.V, dtype=torch.int32, device="cuda")
-        run = lambda: ctx.run_raw(csr.V, csr.E, d[0].data_ptr(), d[1].data_ptr(), d[2].data_ptr(),  # noqa: E731
-                                  d[3].data_ptr(), 4, lab, stage_times=True)
-        ms, _, stats, c = timed_runs(run, stream, args.small_steps, args.warmup, 1)
+        # timed without stage times: reading a dozen event pairs back costs
+        # ~35 us per call, a sixth of this graph's run; the stage split comes
+        # from five more runs right after
+        run = lambda st=False: ctx.run_raw(csr.V, csr.E, d[0].data_ptr(), d[1].data_ptr(),  # noqa: E731
+                                           d[2].data_ptr(), d[3].data_ptr(), 4, lab, stage_times=st)
+        ms, _, _, c = timed_runs(run, stream, args.small_steps, args.warmup, 1)
+        stats = [run(True)[1] for _ in range(5)]
         clk = clk or c
         _, st_x = ctx.run_raw(csr.V, csr.E, d[0].data_ptr(), d[1].data_ptr(), d[2].data_ptr(), d[3].data_ptr(),
                               4, lab, exact_stats=True)
@@ -625,7 +631,7 @@ def bench_web(args):
     ctx.set_stream(stream)
     fb, fa, bb, ba = g.ptrs
     labels = torch.empty(g.V, dtype=torch.int32, device="cuda")
-    tp = autotune.apply(ctx, g.V, g.E)
+    tp = autotune.apply(ctx, g.V, g.E, overrides=args.tuning)
     tun = dict(alpha=tp["alpha"], beta=tp["beta"], gamma=tp["gamma"])
     run = lambda: ctx.run_raw(g.V, g.E, fb, fa, bb, ba, 8, labels, stage_times=True, **tun)  # noqa: E731
     ms, step_ms, stats, clk = timed_runs(run, stream, args.big_steps, args.warmup, 1)
@@ -698,7 +704,7 @@ def bench_batch(args, ws, rank, local):
     ctx = Context(g.V, g.E)
     ctx.set_stream(stream)
     labels = torch.empty(g.V, dtype=torch.int32, device="cuda")
-    tp = autotune.apply(ctx, g.V, g.E, nseg)
+    tp = autotune.apply(ctx, g.V, g.E, nseg, overrides=args.tuning)
     tun = dict(alpha=tp["alpha"], beta=tp["beta"], gamma=tp["gamma"])
     run = lambda: ctx.run_raw(g.V, g.E, fwb, fwa, bwb, bwa, 8, labels, vbase=vb, stage_times=True, **tun)  # noqa: E731
     ms, step_ms, stats, clk = timed_runs(run, stream, args.big_steps, args.warmup, ws)
@@ -721,7 +727,7 @@ def bench_batch(args, ws, rank, local):
             plain = Context(maxv, int(fa.numel()) * 2)
             plain.set_stream(stream)
         out = torch.empty(fb.numel() - 1, dtype=torch.int32, device="cuda")
-        tpp = autotune.apply(plain, int(fb.numel()) - 1, int(fa.numel()))  # tuned like the batch
+        tpp = autotune.apply(plain, int(fb.numel()) - 1, int(fa.numel()), overrides=args.tuning)  # tuned like the batch
         tpl = dict(alpha=tpp["alpha"], beta=tpp["beta"], gamma=tpp["gamma"])
         plain.run(fb, fa, bb, ba, labels_out=out, **tpl)  # warm
         a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -1037,6 +1043,8 @@ def main():
     ap.add_argument("--pool", type=int, default=1024, help="served: distinct graphs in the request pool")
     ap.add_argument("--lanes", type=int, default=4, help="served: concurrent server lanes")
     ap.add_argument("--check-graphs", type=int, default=16, help="served: requested graphs checked")
+    ap.add_argument("--tuning", type=lambda t: dict(kv.split("=") for kv in t.split(",") if kv), default={},
+                    help="launch tunables over the autotuner's, e.g. color_compact=-1,pair_searches=1")
     args = ap.parse_args()
     if args.warmup < 3:
         log("warmup raised to 3 (timing rule)")

@@ -124,6 +124,12 @@ typedef struct {
     int32_t color_pivots;     /* about this many pivots in the first colouring round; doubles per round (1024) */
     int32_t color_compact;    /* colour the large WCCs on a compact copy of their subgraph (dense ids,
                                  only their edges among themselves): 1 on, -1 off (0: default, on) */
+    int32_t pair_searches;    /* run the forward and backward giant searches at the same time (the
+                                 backward one over all active vertices; pivot SCC = both sets'
+                                 intersection): 1 on, -1 off, 0 on for graphs of at most 2^20 vertices */
+    int32_t tiny_residual;    /* solve a residual of at most 1024 vertices (and 4096 edges among them per
+                                 direction) after the giant SCC in one CTA, skipping the later stage
+                                 kernels: -1 off (0: default, on) */
     int32_t reserved;
 } ispan_tuning;
 
@@ -309,12 +315,14 @@ int ispan_scc_small_noalloc(const ispan_csr *g, int32_t *labels_out, void *strea
 int ispan_ref_codes(ispan_ctx *ctx, int32_t *codes_out);
 
 /* Diagnostics: per-level trace of the two reachability searches of the last
- * run, [3][256][4] int64: for the forward (0) and backward (1) search, per
+ * run, [4][256][4] int64: for the forward (0) and backward (1) search, per
  * level, mode (0 top-down, 1 bottom-up, 2 asynchronous), vertices reached,
  * frontier edges, %globaltimer ns; for the large-WCC rounds (2), per round,
  * round number (bits 0-15; grid-wide rounds of its forward search in bits
  * 16-39, of its backward search from bit 40), vertices left, pivots,
- * %globaltimer ns.
+ * %globaltimer ns; and (3), for a run with ISPAN_F_EXACT_STATS, per round,
+ * its forward relaxation's pops, edges checked, vertices queued and ns that
+ * warps waited for work, each summed over all warps.
  * No counterpart in the reference (its VERBOSE "Level-k" lines, src/fw_bw.h:557-572,
  * print the same kind of record). */
 int ispan_debug_trace(ispan_ctx *ctx, int64_t *out, int64_t cap);

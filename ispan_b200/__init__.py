@@ -79,10 +79,10 @@ class Context:
                         1 if on_device else 0)
 
     def set_tuning(self, async_v=0, async_e=0, async_deg=0, bfs_ctas_per_sm=0, color_levels=0,
-                   color_pivots=0, color_compact=0) -> None:
+                   color_pivots=0, color_compact=0, pair_searches=0, tiny_residual=0) -> None:
         """Launch tunables (zero = default); see ispan_b200.autotune."""
         t = _lib.Tuning(int(async_v), int(async_e), int(async_deg), int(bfs_ctas_per_sm), int(color_levels),
-                        int(color_pivots), int(color_compact), 0)
+                        int(color_pivots), int(color_compact), int(pair_searches), int(tiny_residual), 0)
         check(_lib.lib().ispan_ctx_set_tuning(self._h, C.byref(t)), "ispan_ctx_set_tuning")
 
     def tuning(self) -> dict:
@@ -199,14 +199,19 @@ class Context:
 
     def trace(self):
         """Per-level records of the last run: FW and BW searches (mode, reached,
-        frontier_edges, t_ns) and the large-WCC rounds (round, left, pivots, t_ns)."""
-        t = np.zeros(3 * 256 * 4, np.int64)
+        frontier_edges, t_ns), the large-WCC rounds (round, left, pivots, t_ns)
+        and, for a run with exact_stats, each round's relaxation counts (pops,
+        edges, queued, pool-wait ns)."""
+        t = np.zeros(4 * 256 * 4, np.int64)
         check(_lib.lib().ispan_debug_trace(self._h, t.ctypes.data, len(t)), "ispan_debug_trace")
-        t = t.reshape(3, 256, 4)
+        t = t.reshape(4, 256, 4)
         out = []
         for d in range(3):
             rows = [tuple(int(x) for x in r) for r in t[d] if r[3] != 0]
             out.append(rows)
+        # with exact_stats: per colouring round, the forward relaxation's pops,
+        # edges checked, vertices queued and pool-wait ns summed over warps
+        out.append([tuple(int(x) for x in r) for r in t[3][:len(out[2])]])
         return out
 
     def ref_codes(self, V: int) -> np.ndarray:

@@ -32,6 +32,8 @@ TABLE = os.path.join(HERE, "tuning_table.json")
 
 DEFAULTS = {"alpha": 30, "beta": 200, "gamma": 10, "async_v": 65536, "async_e": 262144, "async_deg": 16,
             "bfs_ctas_per_sm": 0, "color_levels": 32, "color_pivots": 1024}
+# switches that are not searched (0 = the library's default; see ispan_tuning)
+SWITCHES = {"color_compact": 0, "pair_searches": 0, "tiny_residual": 0}
 SPACE = {
     "alpha": [5, 10, 30, 100, 300],
     "beta": [50, 200, 1000, 4000],
@@ -68,15 +70,21 @@ def lookup(V: int, E: int, nseg: int = 1, path: str = TABLE) -> dict | None:
     return None if ent is None else {k: ent["params"].get(k, DEFAULTS[k]) for k in DEFAULTS}
 
 
-def apply(ctx, V: int, E: int, nseg: int = 1, path: str = TABLE) -> dict:
-    """Set ctx's tunables for the graph's class; returns the parameters to
-    pass to the run (alpha, beta, gamma) merged with the launch tunables."""
+def apply(ctx, V: int, E: int, nseg: int = 1, path: str = TABLE, overrides: dict | None = None) -> dict:
+    """Set ctx's tunables for the graph's class (then ``overrides``, any of
+    DEFAULTS or SWITCHES); returns the parameters to pass to the run (alpha,
+    beta, gamma) merged with the launch tunables."""
     p = dict(DEFAULTS)
+    p.update(SWITCHES)
     t = lookup(V, E, nseg, path)
     if t:
         p.update(t)
+    for k, v in (overrides or {}).items():
+        if k not in p:
+            raise KeyError(f"unknown tunable {k!r}")
+        p[k] = int(v)
     ctx.set_tuning(p["async_v"], p["async_e"], p["async_deg"], p["bfs_ctas_per_sm"], p["color_levels"],
-                   p["color_pivots"])
+                   p["color_pivots"], p["color_compact"], p["pair_searches"], p["tiny_residual"])
     return p
 
 

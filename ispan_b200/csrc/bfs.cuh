@@ -29,7 +29,11 @@
 // exceeds gamma; TD <-> TAIL on the frontier size.
 //
 // DIR 0 (forward):  visit map F, restricted to A, expands out-edges.
-// DIR 1 (backward): visit map B, restricted to F, expands in-edges.
+// DIR 1 (backward): visit map B, restricted to F, expands in-edges -- or,
+// when both searches run at the same time (kRunPair; small graphs, whose
+// levels are latency-bound), restricted to A, in its own queues, with its
+// own grid barrier and the map D for its bottom-up snapshots.  The pivot SCC
+// is F & B either way.
 #pragma once
 #include "common.cuh"
 
@@ -41,6 +45,7 @@ constexpr int kAsyncDeg = 16;           // default of Run::async_deg: vertices u
 constexpr int kAsyncMaxLevels = 4096;   // local levels before a CTA hands its frontier back
 constexpr int64_t kAsyncV = 65536;      // defaults of Run::async_v: frontier size that enters the async mode ...
 constexpr int64_t kAsyncE = 262144;     // ... and Run::async_e: frontier edges
+constexpr int64_t kPairMaxV = 1 << 20;  // graphs up to this many vertices run their two searches at once
 
 enum BfsMode : int { M_TD = 0, M_BU = 1, M_ASYNC = 2, M_DONE = 3 };
 
@@ -65,7 +70,8 @@ struct BfsDir {
             R = r.A; Vm = r.F;
         } else {
             xbeg = r.bw_beg; xadj = r.bw_adj; pbeg = r.fw_beg; padj = r.fw_adj; obeg = r.fw_beg;
-            R = r.F; Vm = r.B;
+            R = (r.flags & kRunPair) ? r.A : r.F;
+            Vm = r.B;
         }
     }
     __device__ __forceinline__ int64_t xdeg(int64_t v) const { return ld_off(xbeg, v + 1) - ld_off(xbeg, v); }
@@ -501,8 +507,11 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Run<OffT> r, BfsCtl *ctl) {
     (void)ctl;
 
     // budget for the alpha rule: unexplored expansion-side edges
-    int64_t m_unexpl = (int64_t)(DIR == 0 ? r.counters[C_MU0] : r.counters[C_FW_MU]);
-    const int64_t n_total = (int64_t)(DIR == 0 ? r.counters[C_ACTIVE0] : r.counters[C_FW_SIZE]);
+    // (a backward search over A, running beside the forward one, takes the
+    // active set's figures: the forward search's are not known yet)
+    const bool over_a = DIR == 0 || (r.flags & kRunPair);
+    int64_t m_unexpl = (int64_t)(DIR == 0 ? r.counters[C_MU0] : over_a ? r.counters[C_MU0_IN] : r.counters[C_FW_MU]);
+    const int64_t n_total = (int64_t)(over_a ? r.counters[C_ACTIVE0] : r.counters[C_FW_SIZE]);
     int level = 0, mode = M_TD;
     bool left_bu = false;  // like the reference, a search never returns to bottom-up
     int64_t total_vis = 0;

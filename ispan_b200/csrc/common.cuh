@@ -62,7 +62,7 @@ struct Run {
     unsigned long long *counters; // [kNumCounters] statistics
     int64_t *hist;                // [kHistCap] SCC size histogram (sizes < cap)
     unsigned int *gsync;          // [kGridSyncWords] grid barrier (count at 0, generation at kGenWord)
-    long long *trace;             // [2][kTraceLevels][4] per-level BFS trace (diagnostics)
+    long long *trace;             // [4][kTraceLevels][4] diagnostics: FW and BW levels, colouring rounds, their pops
     int *err;                     // [4] error word, detail
     int32_t alpha, beta, gamma;
     uint32_t flags;
@@ -99,6 +99,7 @@ enum Counter {
     C_Q1_XDEG,       // sum of out+in degrees over the peel's worklist (residual after the giant)
     C_Q2_N,          // vertices left after the first peel (trim-2/3 worklist)
     C_Q2_XDEG,       // sum of their out+in degrees
+    C_MU0_IN,        // sum of in-degrees of the active vertices (budget of a backward search over A)
     kNumCounters = 32
 };
 constexpr int kHistCap = 1 << 16;   // exact histogram for SCC sizes below this
@@ -107,6 +108,11 @@ constexpr int kBigCap = 1 << 16;    // list of larger SCC sizes (hist[kHistCap..
 
 // error codes mirror ispan_b200.h
 constexpr int kErrTimeout = ISPAN_ERR_TIMEOUT;
+
+// Internal run flag (never one of the caller's ISPAN_F_* bits): the two
+// searches run at the same time, the backward one over the whole active map
+// instead of inside the forward set; the pivot SCC is then F & B.
+constexpr uint32_t kRunPair = 1u << 30;
 constexpr int kErrOverflow = ISPAN_ERR_INTERNAL;
 
 // ---------------------------------------------------------------------------

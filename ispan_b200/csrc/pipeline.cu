@@ -26,6 +26,7 @@
 #include "bfs.cuh"
 #include "pack.cuh"
 #include "compact.cuh"
+#include "tiny.cuh"
 #include "lane.h"
 #include "stages.cuh"
 
@@ -148,11 +149,16 @@ struct ispan_ctx {
     unsigned long long *h_counters = nullptr;  // pinned
     int *h_err = nullptr;
 
-    ispan_tuning tuning = {0, 0, 0, 0, 0, 0, 0, 0};
+    ispan_tuning tuning = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
 
     // launch geometry
     int g_stream = 0;           // grid for plain grid-stride kernels
     int g_coop[5] = {0, 0, 0, 0, 0};  // bfs<0>, bfs<1>, trim1, color, color on the compact graph
+    int g_pair = 0;             // each search's grid when the two run at the same time
+
+    // the backward search's stream when the searches run at the same time
+    cudaStream_t stream2 = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     int g_coop_w = 0;           // offset width the coop grids were computed for
 
     // CUDA graph cache
@@ -173,6 +179,7 @@ struct ispan_ctx {
 
 static int64_t words_of(int64_t V) { return (V + 31) / 32 + 1; }
 
+static constexpr int64_t kL2WindowMinBytes = 4 << 20;  // status maps smaller than this get no L2 window
 static constexpr int kCtlCounters = 0;                       // kNumCounters
 static constexpr int kCtlQpk = kNumCounters;                 // 3 (forward search)
 static constexpr int kCtlLvl = kNumCounters + 4;             // 12
@@ -240,10 +247,10 @@ static int ctx_alloc(ispan_ctx *c) {
     rc |= dalloc(&c->small, V, o, g);
     rc |= dalloc(&c->ctlblk, kCtlTotal, o, g);
     rc |= dalloc(&c->hist, kHistCap + kBigCap, o, g);
-    rc |= dalloc(&c->gsync, kGridSyncWords, o, g);
+    rc |= dalloc(&c->gsync, 2 * kGridSyncWords, o, g);  // the second block: a backward search run beside
     rc |= dalloc(&c->err, 4, o, g);
     rc |= dalloc(&c->bfsctl, 1, o, g);
-    rc |= dalloc(&c->trace, 3 * kTraceLevels * 4, o, g);
+    rc |= dalloc(&c->trace, 4 * kTraceLevels * 4, o, g);
     return rc ? ISPAN_ERR_NOMEM : ISPAN_OK;
 }
 
@@ -325,7 +332,7 @@ static void fill_run(ispan_ctx *c, Run<OffT> &r, Ext<OffT> &x, int64_t V, int64_
     r.alpha = p && p->alpha > 0 ? p->alpha : 30;
     r.beta = p && p->beta > 0 ? p->beta : 200;
     r.gamma = p && p->gamma > 0 ? p->gamma : 10;
-    r.flags = p ? p->flags : 0;
+    r.flags = (p ? p->flags : 0) & ~kRunPair;  // set by enqueue when the searches run together
     r.async_v = c->tuning.async_v > 0 ? c->tuning.async_v : kAsyncV;
     r.async_e = c->tuning.async_e > 0 ? c->tuning.async_e : kAsyncE;
     r.async_deg = c->tuning.async_deg > 0 ? c->tuning.async_deg : kAsyncDeg;
@@ -409,6 +416,22 @@ static cudaError_t launch_coop(Kern k, int grid, cudaStream_t s, Args... args) {
     return cudaLaunchCooperativeKernel((const void *)k, dim3(grid), dim3(kBlock), ptrs, 0, s);
 }
 
+// Whether the two searches of a run go at the same time.  On a small graph
+// each search level costs a few microseconds of dependent loads and a grid
+// barrier whatever its work, so running the backward search beside the
+// forward one (over the active map, pivot SCC = F & B) halves the levels in
+// sequence; on a large graph the backward search inside F does less work.
+// The backward search then takes buffers that are free until the giant is
+// done: the colouring lists as its vertex queues, the worklist block as its
+// edge prefixes, the peel counters as its chunk maps, D for its snapshots.
+template <typename OffT>
+static bool pair_searches(const ispan_ctx *c, const Run<OffT> &r) {
+    const int t = c->tuning.pair_searches;
+    if (t < 0 || !c->stream2 || c->g_pair < 1) return false;
+    if (r.E / kChunk + 4 > c->maxV + 32) return false;  // chunk maps must fit the peel counters
+    return t > 0 || r.V <= kPairMaxV;
+}
+
 // Enqueue the whole pipeline on c->stream (plain launches; may be captured).
 template <typename OffT>
 static cudaError_t enqueue(ispan_ctx *c, Run<OffT> r, Ext<OffT> x, bool times, bool capturing) {
@@ -416,6 +439,8 @@ static cudaError_t enqueue(ispan_ctx *c, Run<OffT> r, Ext<OffT> x, bool times, b
     const int G = c->g_stream;
     unsigned long long *ctl = c->ctlblk;
     cudaError_t e;
+    const bool pair = pair_searches(c, r);
+    if (pair) r.flags |= kRunPair;
 #define EV(i) \
     if (times) { e = cudaEventRecordWithFlags(c->ev[i], s, capturing ? cudaEventRecordExternal : 0); if (e) return e; }
 #define LK(...) \
@@ -425,9 +450,9 @@ static cudaError_t enqueue(ispan_ctx *c, Run<OffT> r, Ext<OffT> x, bool times, b
         ResetDesc rd;
         rd.z[0] = {ctl, (int64_t)kCtlTotal * 8};
         rd.z[1] = {c->hist, (int64_t)(kHistCap + kBigCap) * 8};
-        rd.z[2] = {c->gsync, kGridSyncWords * 4};
+        rd.z[2] = {c->gsync, 2 * kGridSyncWords * 4};
         rd.z[3] = {c->err, 4 * 4};
-        rd.z[4] = {c->trace, 3 * kTraceLevels * 4 * 8};
+        rd.z[4] = {c->trace, 4 * kTraceLevels * 4 * 8};
         rd.z[5] = {c->pivot_key, r.nseg * 8};
         rd.z[6] = {c->gsize, r.nseg * 8};
         rd.gmin = c->gmin;
@@ -436,19 +461,44 @@ static cudaError_t enqueue(ispan_ctx *c, Run<OffT> r, Ext<OffT> x, bool times, b
     }
     LK((k_trim1_first<OffT><<<G, kBlock, 0, s>>>(r, x)));
     EV(1);
-    LK((k_seed<OffT, 0><<<std::max<int64_t>(1, (r.nseg + 1023) / 1024), 32 * 32, 0, s>>>(r)));
-    if ((e = launch_coop(k_bfs<OffT, 0>, c->g_coop[0], s, r, c->bfsctl))) return e;
-    EV(2);
+    const int gseed = (int)std::max<int64_t>(1, (r.nseg + 1023) / 1024);
     Run<OffT> rb = r;  // the backward search counts in its own queue and level slots
     rb.qpk = ctl + kCtlQpkB;
     rb.lvl = ctl + kCtlLvlB;
-    LK((k_seed<OffT, 1><<<std::max<int64_t>(1, (r.nseg + 1023) / 1024), 32 * 32, 0, s>>>(rb)));
-    if ((e = launch_coop(k_bfs<OffT, 1>, c->g_coop[1], s, rb, c->bfsctl))) return e;
+    if (pair) {
+        const int64_t Vp = c->maxV + 32;  // entries of each scratch array
+        rb.qv[0] = c->large[0];
+        rb.qv[1] = c->large[1];
+        rb.qe[0] = reinterpret_cast<int64_t *>(c->wl4);
+        rb.qe[1] = reinterpret_cast<int64_t *>(c->wl4 + 2 * Vp);
+        rb.qchunk[0] = c->cnt_out;
+        rb.qchunk[1] = c->cnt_in;
+        rb.P = c->D;
+        rb.gsync = c->gsync + kGridSyncWords;
+        LK((k_seed<OffT, 0><<<gseed, 32 * 32, 0, s>>>(r)));
+        LK((k_seed<OffT, 1><<<gseed, 32 * 32, 0, s>>>(rb)));
+        if ((e = cudaEventRecord(c->ev_fork, s))) return e;
+        if ((e = cudaStreamWaitEvent(c->stream2, c->ev_fork, 0))) return e;
+        if ((e = launch_coop(k_bfs<OffT, 1>, c->g_pair, c->stream2, rb, c->bfsctl))) return e;
+        if ((e = launch_coop(k_bfs<OffT, 0>, c->g_pair, s, r, c->bfsctl))) return e;
+        EV(2);
+        if ((e = cudaEventRecord(c->ev_join, c->stream2))) return e;
+        if ((e = cudaStreamWaitEvent(s, c->ev_join, 0))) return e;
+    } else {
+        LK((k_seed<OffT, 0><<<gseed, 32 * 32, 0, s>>>(r)));
+        if ((e = launch_coop(k_bfs<OffT, 0>, c->g_coop[0], s, r, c->bfsctl))) return e;
+        EV(2);
+        LK((k_seed<OffT, 1><<<gseed, 32 * 32, 0, s>>>(rb)));
+        if ((e = launch_coop(k_bfs<OffT, 1>, c->g_coop[1], s, rb, c->bfsctl))) return e;
+    }
     if (r.flags & ISPAN_F_EXACT_STATS) LK((k_reach_degrees<OffT><<<G, kBlock, 0, s>>>(r)));
     EV(3);
     LK((k_giant_residual<OffT><<<G, kBlock, 0, s>>>(r, x)));
     if (r.flags & ISPAN_F_EXACT_STATS) LK((k_list_degrees<OffT><<<G, kBlock, 0, s>>>(r, r.wl[0], x.ctl + K_WL0, -1, C_Q1_XDEG)));
     EV(4);
+    // a residual of at most kTinyV vertices is solved here in one CTA, and
+    // every stage kernel up to the finalisation then returns at once
+    if (c->tuning.tiny_residual >= 0) LK((k_tiny_residual<OffT><<<1, kBlock, 0, s>>>(r, x)));
     if ((e = launch_coop(k_trim1<OffT>, c->g_coop[2], s, r, x, 0, 1, 1))) return e;
     if (r.flags & ISPAN_F_EXACT_STATS) LK((k_list_degrees<OffT><<<G, kBlock, 0, s>>>(r, r.wl[1], x.ctl + K_WL1, C_Q2_N, C_Q2_XDEG)));
     EV(5);
@@ -519,6 +569,8 @@ static int coop_setup(ispan_ctx *c) {
     const int want = c->tuning.bfs_ctas_per_sm;
     if (want > 0)
         for (int i = 0; i < 2; ++i) c->g_coop[i] = std::min(c->g_coop[i], want * nsm);
+    // two searches at the same time: each on half of what both can keep resident
+    c->g_pair = std::max(1, std::min(c->g_coop[0], c->g_coop[1]) / 2);
     c->g_coop[2] = coop_grid(k_trim1<OffT>, nsm, kBlock);
     c->g_coop[3] = coop_grid(k_color<OffT>, nsm, kBlock);
     c->g_coop[4] = coop_grid(k_color<int32_t>, nsm, kBlock);
@@ -604,7 +656,9 @@ static int run_t(ispan_ctx *c, int64_t V, int64_t E, int32_t nseg, const OffT *f
     // stage events are always recorded (they are nodes of the captured graph);
     // they are read back only when the caller asks for stage times
     const bool times = (flags & ISPAN_F_STAGE_TIMES) && st;
-    const bool l2win = !(flags & ISPAN_F_NO_L2_WINDOW);
+    // the window pays only for maps larger than what stays in L2 anyway; on
+    // small graphs its attribute calls would cost more than the run's stages
+    const bool l2win = !(flags & ISPAN_F_NO_L2_WINDOW) && 6 * r.W * 4 >= kL2WindowMinBytes;
     if (l2win) l2_window(c, true);
     bool use_graph = !(flags & ISPAN_F_NO_GRAPH) && !c->graph_broken;
     if (use_graph) {
@@ -1145,6 +1199,10 @@ int ispan_ctx_create(int device, int64_t max_V, int64_t max_E, ispan_ctx **out) 
     if (!rc) rc = ctx_segments(c, 1);
     if (!rc && cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) rc = ISPAN_ERR_CUDA;
     c->own_stream = true;
+    if (!rc && cudaStreamCreateWithFlags(&c->stream2, cudaStreamNonBlocking) != cudaSuccess) rc = ISPAN_ERR_CUDA;
+    if (!rc && (cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+                cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming) != cudaSuccess))
+        rc = ISPAN_ERR_CUDA;
     if (!rc && cudaMallocHost(&c->h_counters, kNumCounters * sizeof(unsigned long long)) != cudaSuccess)
         rc = ISPAN_ERR_NOMEM;
     if (!rc && cudaMallocHost(&c->h_err, 4 * sizeof(int)) != cudaSuccess) rc = ISPAN_ERR_NOMEM;
@@ -1182,6 +1240,12 @@ int ispan_ctx_destroy(ispan_ctx *c) {
         for (int i = 0; i < kNumEv; ++i) cudaEventDestroy(c->ev[i]);
     if (c->h_counters) cudaFreeHost(c->h_counters);
     if (c->h_err) cudaFreeHost(c->h_err);
+    if (c->stream2) {
+        cudaStreamSynchronize(c->stream2);
+        cudaStreamDestroy(c->stream2);
+    }
+    if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+    if (c->ev_join) cudaEventDestroy(c->ev_join);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return ISPAN_OK;
@@ -1206,7 +1270,7 @@ int ispan_ctx_set_tuning(ispan_ctx *c, const ispan_tuning *t) {
               t->color_pivots < 0))
         return ISPAN_ERR_ARG;
     std::lock_guard<std::mutex> lock(c->mu);
-    c->tuning = t ? *t : ispan_tuning{0, 0, 0, 0, 0, 0, 0, 0};
+    c->tuning = t ? *t : ispan_tuning{0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
     c->g_coop_w = 0;  // recompute the persistent grids
     if (c->gexec) {   // the captured graph holds the old values
         cudaGraphExecDestroy(c->gexec);
@@ -1225,6 +1289,8 @@ int ispan_ctx_get_tuning(ispan_ctx *c, ispan_tuning *t) {
     t->color_levels = c->tuning.color_levels > 0 ? c->tuning.color_levels : kCLevels;
     t->color_pivots = c->tuning.color_pivots > 0 ? c->tuning.color_pivots : kCPivots;
     t->color_compact = c->tuning.color_compact >= 0 ? 1 : -1;
+    t->pair_searches = c->tuning.pair_searches;
+    t->tiny_residual = c->tuning.tiny_residual >= 0 ? 1 : -1;
     t->reserved = 0;
     return ISPAN_OK;
 }
@@ -1313,7 +1379,7 @@ int ispan_debug_barrier_timeout(ispan_ctx *c, int64_t limit_us) {
 int ispan_debug_trace(ispan_ctx *c, int64_t *out, int64_t cap) {
     if (!c || !out) return ISPAN_ERR_ARG;
     std::lock_guard<std::mutex> lock(c->mu);
-    int64_t n = std::min<int64_t>(cap, 3 * kTraceLevels * 4);
+    int64_t n = std::min<int64_t>(cap, 4 * kTraceLevels * 4);
     CK(cudaMemcpy(out, c->trace, n * sizeof(int64_t), cudaMemcpyDeviceToHost));
     return ISPAN_OK;
 }

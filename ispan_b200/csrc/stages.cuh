@@ -23,6 +23,7 @@ enum Ctl64 {
     K_SPILL, K_MICE_SCC, K_LOCAL_NEXT, K_MINPRIO0, K_MINPRIO1, K_CAND,
     K_CMP_OK, K_CMP_EF, K_CMP_EB,  // compact colouring graph: built (1), its edge counts
     K_WCC_GIANT,                   // (root << 32) | 1 when one WCC holds half the root sample
+    K_TINY,                        // 1: k_tiny_residual solved the residual; later stages return at once
     kNumCtl = 32
 };
 
@@ -143,7 +144,7 @@ __global__ void __launch_bounds__(kBlock) k_trim1_first(Run<OffT> r, Ext<OffT> x
     const int lane = lane_id();
     const int64_t gw = ((int64_t)blockIdx.x * kBlock + threadIdx.x) >> 5;
     const int64_t nw = (int64_t)gridDim.x * kWarps;
-    int64_t n_act = 0, mu = 0, n_tr = 0;
+    int64_t n_act = 0, mu = 0, mui = 0, n_tr = 0;
     unsigned long long best = 0;
     for (int64_t wb = gw * U; wb < r.W; wb += nw * U) {
         int64_t od[U], id[U];
@@ -174,6 +175,7 @@ __global__ void __launch_bounds__(kBlock) k_trim1_first(Run<OffT> r, Ext<OffT> x
             if (act) {
                 ++n_act;
                 mu += od[j];
+                mui += id[j];
                 unsigned long long prod = (unsigned long long)od[j] * (unsigned long long)id[j];
                 if (prod > 0xffffffffull) prod = 0xffffffffull;
                 key = (prod << 32) | (0xffffffffull - (unsigned long long)v);
@@ -201,10 +203,11 @@ __global__ void __launch_bounds__(kBlock) k_trim1_first(Run<OffT> r, Ext<OffT> x
         best = warp_max_u64(best);
         if (lane == 0 && best) atomicMax(r.pivot_key, best);
     }
-    int64_t a = block_sum64(n_act, sh), m = block_sum64(mu, sh), t = block_sum64(n_tr, sh);
+    int64_t a = block_sum64(n_act, sh), m = block_sum64(mu, sh), mi = block_sum64(mui, sh), t = block_sum64(n_tr, sh);
     if (threadIdx.x == 0) {
         if (a) atomicAdd(r.counters + C_ACTIVE0, (unsigned long long)a);
         if (m) atomicAdd(r.counters + C_MU0, (unsigned long long)m);
+        if (mi) atomicAdd(r.counters + C_MU0_IN, (unsigned long long)mi);
         if (t) atomicAdd(r.counters + C_TRIM1, (unsigned long long)t);
     }
 }
@@ -238,7 +241,8 @@ __global__ void k_seed(Run<OffT> r) {
     }
 }
 
-// The pivot SCC of each graph is B (reached backward inside F).  One pass
+// The pivot SCC of each graph is B (reached backward inside F; F & B when
+// the searches ran at the same time).  One pass
 // over the maps: B leaves the active map, each graph's minimum member id (its
 // canonical label, written by k_finalize) and size are taken, and the
 // remaining active vertices are compacted into the residual worklist.  Each
@@ -255,8 +259,14 @@ __global__ void __launch_bounds__(kBlock) k_giant_residual(Run<OffT> r, Ext<OffT
     int64_t n_giant = 0, n_res = 0;
     int gm = 0x7fffffff;
     // pass 1: update A, giant stats, count the residual
+    const bool pair = (r.flags & kRunPair) != 0;
     for (int64_t wi = w0 + tid; wi < w1; wi += kBlock) {
         uint32_t a = r.A[wi], b = r.B[wi];
+        if (pair) {  // the backward search ran over A: the pivot SCC is F & B; D held its snapshots
+            b &= r.F[wi];
+            r.B[wi] = b;
+            r.D[wi] = 0u;
+        }
         uint32_t res = a & ~b;
         if (b) r.A[wi] = res;
         n_res += __popc(res);
@@ -353,6 +363,7 @@ __device__ __forceinline__ void count_active(const OffT *beg, const int32_t *adj
 
 template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_trim1(Run<OffT> r, Ext<OffT> x, int in, int out, int cand) {
+    if (__ldcg(x.ctl + K_TINY)) return;  // the residual was solved in one CTA
     __shared__ int64_t sh[kWarps];
     const int64_t gt = (int64_t)blockIdx.x * kBlock + threadIdx.x;
     const int64_t nt = (int64_t)gridDim.x * kBlock;
@@ -512,6 +523,7 @@ __device__ __forceinline__ bool claim(Run<OffT> &r, Ext<OffT> &x, int32_t v, int
 template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_trim2(Run<OffT> r, Ext<OffT> x, const int32_t *wl,
                                                   const unsigned long long *n_wl) {
+    if (__ldcg(x.ctl + K_TINY)) return;  // the residual was solved in one CTA
     __shared__ int64_t sh[kWarps];
     const int64_t n = (int64_t)__ldcg(n_wl);
     int64_t got = 0;
@@ -540,6 +552,7 @@ __global__ void __launch_bounds__(kBlock) k_trim2(Run<OffT> r, Ext<OffT> x, cons
 template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_trim3(Run<OffT> r, Ext<OffT> x, const int32_t *wl,
                                                   const unsigned long long *n_wl) {
+    if (__ldcg(x.ctl + K_TINY)) return;  // the residual was solved in one CTA
     __shared__ int64_t sh[kWarps];
     const int64_t n = (int64_t)__ldcg(n_wl);
     int64_t got = 0;
@@ -606,6 +619,7 @@ __device__ __forceinline__ int32_t uf_root(const int32_t *parent, int32_t x) {
 
 template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_wcc_init(Run<OffT> r, Ext<OffT> x, int in) {
+    if (__ldcg(x.ctl + K_TINY)) return;  // the residual was solved in one CTA
     const int64_t n = (int64_t)__ldcg(x.ctl + K_WL0 + in);
     for (int64_t i = (int64_t)blockIdx.x * kBlock + threadIdx.x; i < n; i += (int64_t)gridDim.x * kBlock) {
         int32_t v = r.wl[in][i];
@@ -658,6 +672,7 @@ constexpr int64_t kWccSkipMin = 1 << 14;  // smaller worklists: no sample, every
 
 template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_wcc_hook(Run<OffT> r, Ext<OffT> x, int in, int phase) {
+    if (__ldcg(x.ctl + K_TINY)) return;  // the residual was solved in one CTA
     const int64_t n = (int64_t)__ldcg(x.ctl + K_WL0 + in);
     const bool skip_giant = phase == 1 && __ldcg(x.ctl + K_WCC_GIANT) != 0;
     const int32_t g = (int32_t)(__ldcg(x.ctl + K_WCC_GIANT) >> 32);
@@ -681,6 +696,7 @@ __global__ void __launch_bounds__(kBlock) k_wcc_hook(Run<OffT> r, Ext<OffT> x, i
 // vertices and records the most frequent one if it holds half the sample
 template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_wcc_compress(Run<OffT> r, Ext<OffT> x, int in) {
+    if (__ldcg(x.ctl + K_TINY)) return;  // the residual was solved in one CTA
     const int64_t n = (int64_t)__ldcg(x.ctl + K_WL0 + in);
     for (int64_t i = (int64_t)blockIdx.x * kBlock + threadIdx.x; i < n; i += (int64_t)gridDim.x * kBlock) {
         const int32_t v = r.wl[in][i];
@@ -690,6 +706,7 @@ __global__ void __launch_bounds__(kBlock) k_wcc_compress(Run<OffT> r, Ext<OffT> 
 
 template <typename OffT>
 __global__ void __launch_bounds__(kWccRootSamples) k_wcc_giant(Run<OffT> r, Ext<OffT> x, int in) {
+    if (__ldcg(x.ctl + K_TINY)) return;  // the residual was solved in one CTA
     __shared__ int32_t roots[kWccRootSamples];
     __shared__ int best, best_n;
     const int64_t n = (int64_t)__ldcg(x.ctl + K_WL0 + in);
@@ -717,6 +734,7 @@ __global__ void __launch_bounds__(kWccRootSamples) k_wcc_giant(Run<OffT> r, Ext<
 // flatten, count members per root, list the roots
 template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_wcc_flatten(Run<OffT> r, Ext<OffT> x, int in) {
+    if (__ldcg(x.ctl + K_TINY)) return;  // the residual was solved in one CTA
     const int64_t n = (int64_t)__ldcg(x.ctl + K_WL0 + in);
     for (int64_t i = (int64_t)blockIdx.x * kBlock + threadIdx.x; i - threadIdx.x < n;
          i += (int64_t)gridDim.x * kBlock) {
@@ -738,6 +756,7 @@ __global__ void __launch_bounds__(kBlock) k_wcc_flatten(Run<OffT> r, Ext<OffT> x
 // Reserve member space for small WCCs; route the rest to the large path.
 template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_wcc_alloc(Run<OffT> r, Ext<OffT> x) {
+    if (__ldcg(x.ctl + K_TINY)) return;  // the residual was solved in one CTA
     const int64_t n = (int64_t)__ldcg(x.ctl + K_ROOTS);
     for (int64_t i = (int64_t)blockIdx.x * kBlock + threadIdx.x; i - threadIdx.x < n;
          i += (int64_t)gridDim.x * kBlock) {
@@ -758,6 +777,7 @@ __global__ void __launch_bounds__(kBlock) k_wcc_alloc(Run<OffT> r, Ext<OffT> x) 
 
 template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_wcc_scatter(Run<OffT> r, Ext<OffT> x, int in) {
+    if (__ldcg(x.ctl + K_TINY)) return;  // the residual was solved in one CTA
     const int64_t n = (int64_t)__ldcg(x.ctl + K_WL0 + in);
     for (int64_t i = (int64_t)blockIdx.x * kBlock + threadIdx.x; i - threadIdx.x < n;
          i += (int64_t)gridDim.x * kBlock) {
@@ -789,6 +809,7 @@ constexpr int kLocalThreads = 256;
 
 template <typename OffT>
 __global__ void __launch_bounds__(kLocalThreads) k_local_scc(Run<OffT> r, Ext<OffT> x) {
+    if (__ldcg(x.ctl + K_TINY)) return;  // the residual was solved in one CTA
     __shared__ int32_t gid[kLocalV];
     __shared__ int32_t loff[kLocalV + 1];
     __shared__ uint16_t ladj[kLocalE];
@@ -1108,7 +1129,7 @@ __device__ __forceinline__ void cta_unlock(int *l) {
 template <typename OffT, int KIND>
 __device__ __forceinline__ void color_async_round(const Run<OffT> &r, const Ext<OffT> &x, const int32_t *q_in,
                                                   int64_t n_in, int32_t *q_out, unsigned long long *n_out,
-                                                  ColorSmem &sm) {
+                                                  ColorSmem &sm, long long *cst) {
     unsigned long long *cc = reinterpret_cast<unsigned long long *>(r.qe[0]);  // class | colour | flag
     int32_t *rootof = r.aux2;
     const OffT *beg = KIND == 0 ? r.fw_beg : r.bw_beg;
@@ -1129,6 +1150,7 @@ __device__ __forceinline__ void color_async_round(const Run<OffT> &r, const Ext<
     int head = 0, tail = 0;  // ring [head, tail), warp-uniform
     const int cap = 4 * r.color_levels;
     bool capped = false;
+    long long st_pops = 0, st_edges = 0, st_push = 0, st_wait = 0;  // diagnostics (cst set)
     for (int chunk = 0;; ++chunk) {
         if (chunk >= cap) { capped = true; break; }
         int nb = 0;
@@ -1150,6 +1172,7 @@ __device__ __forceinline__ void color_async_round(const Run<OffT> &r, const Ext<
                 if (lane == 0) {
                     bool idle = false;
                     const uint64_t t0 = globaltimer();
+                    if (cst) st_wait -= (long long)t0;
                     for (int it = 0;; ++it) {
                         // test without the lock first: waiting warps poll, the lock
                         // stays free for the warps that feed the pool
@@ -1175,6 +1198,7 @@ __device__ __forceinline__ void color_async_round(const Run<OffT> &r, const Ext<
                         }
                         __nanosleep(64);
                     }
+                    if (cst) st_wait += (long long)globaltimer();
                 }
                 got = __shfl_sync(kFull, got, 0);
                 if (got == 0) break;  // nothing left in this CTA for this round
@@ -1206,6 +1230,8 @@ __device__ __forceinline__ void color_async_round(const Run<OffT> &r, const Ext<
         }
         const int64_t total = __shfl_sync(kFull, incl, 31);
         base -= incl - deg;  // edge index of the chunk's k-th edge, k in this lane's range: base + k
+        st_pops += nb;
+        st_edges += total;
         for (int64_t k0 = 0; k0 < total; k0 += 64) {
             int32_t w[2], vo[2];
             unsigned long long po[2], pw[2];
@@ -1256,6 +1282,7 @@ __device__ __forceinline__ void color_async_round(const Run<OffT> &r, const Ext<
                 const unsigned m = __ballot_sync(kFull, push);
                 if (m) {
                     const int cnt = __popc(m), rank = __popc(m & lt);
+                    st_push += cnt;
                     bool placed = false;
                     // one read, broadcast: the branch below must be warp-uniform
                     const int act = __shfl_sync(kFull, ld_volatile_int(&sm.active), 0);
@@ -1307,6 +1334,12 @@ __device__ __forceinline__ void color_async_round(const Run<OffT> &r, const Ext<
                 if (VOK((long long)(g + i), 18)) q_out[g + i] = ring[(head + i) & (kCWQ - 1)];
         }
     }
+    if (cst && lane == 0) {
+        atomicAdd((unsigned long long *)cst + 0, (unsigned long long)st_pops);
+        atomicAdd((unsigned long long *)cst + 1, (unsigned long long)st_edges);
+        atomicAdd((unsigned long long *)cst + 2, (unsigned long long)st_push);
+        atomicAdd((unsigned long long *)cst + 3, (unsigned long long)st_wait);
+    }
     __syncthreads();
     // the unread rest of the slice (left by warps that reached their chunk
     // cap) and what is left in the pool go back to the grid queue
@@ -1330,13 +1363,13 @@ __device__ __forceinline__ void color_async_round(const Run<OffT> &r, const Ext<
 // failed.
 template <typename OffT, int KIND>
 __device__ __forceinline__ int color_async(const Run<OffT> &r, const Ext<OffT> &x, const int32_t *q0, int64_t n0,
-                                           unsigned long long *cqc, ColorSmem &sm) {
+                                           unsigned long long *cqc, ColorSmem &sm, long long *cst = nullptr) {
     for (int lv = 0; lv < (1 << 30); ++lv) {
         const int64_t n = lv == 0 ? n0 : (int64_t)__ldcg(cqc + lv % 3);
         if (n == 0) return lv;
         if (blockIdx.x == 0 && threadIdx.x == 0) cqc[(lv + 2) % 3] = 0ull;
         const int32_t *q = lv == 0 ? q0 : x.cq[lv & 1];
-        color_async_round<OffT, KIND>(r, x, q, n, x.cq[(lv + 1) & 1], cqc + (lv + 1) % 3, sm);
+        color_async_round<OffT, KIND>(r, x, q, n, x.cq[(lv + 1) & 1], cqc + (lv + 1) % 3, sm, cst);
         if (!grid_sync(r.gsync, r.err)) return -1;
         if (lv > 64 * (r.V + 2)) {  // colours only decrease; more rounds is a bug
             if (threadIdx.x == 0) atomicCAS(r.err, 0, kErrOverflow);
@@ -1425,7 +1458,12 @@ __global__ void __launch_bounds__(kBlock, 2) k_color(Run<OffT> r, Ext<OffT> x) {
         // forward min-colour relaxation from the pivots; cqc[0] is freed by
         // color_async only after every CTA has read it here
         const int64_t npiv = (int64_t)__ldcg(cqc + 0);
-        const int fw_rounds = color_async<OffT, 0>(r, x, x.cq[0], npiv, cqc, sm);
+        // diagnostics on request (exact statistics): pops, edges, pushes and
+        // pool-wait time of the forward relaxation, summed over warps
+        long long *cst = (r.flags & ISPAN_F_EXACT_STATS) && rounds <= kTraceLevels
+                             ? r.trace + ((long long)3 * kTraceLevels + rounds - 1) * 4
+                             : nullptr;
+        const int fw_rounds = color_async<OffT, 0>(r, x, x.cq[0], npiv, cqc, sm, cst);
         if (fw_rounds < 0) return;
         if (blockIdx.x == 0 && threadIdx.x == 0) { cqc[0] = 0; cqc[1] = 0; cqc[2] = 0; }
         if (!grid_sync(r.gsync, r.err)) return;

@@ -29,9 +29,18 @@ def test_lookup_and_apply(tmp_path):
     ctx = FakeCtx()
     got = AT.apply(ctx, 65_536, 955_000, path=str(p))
     assert got["alpha"] == 100 and ctx.calls == [(4096, AT.DEFAULTS["async_e"], AT.DEFAULTS["async_deg"], 1,
-                                                  AT.DEFAULTS["color_levels"], AT.DEFAULTS["color_pivots"])]
+                                                  AT.DEFAULTS["color_levels"], AT.DEFAULTS["color_pivots"],
+                                                  0, 0, 0)]
     ctx = FakeCtx()
-    assert AT.apply(ctx, 10, 10, path=str(p)) == AT.DEFAULTS  # untuned class: defaults
+    assert AT.apply(ctx, 10, 10, path=str(p)) == dict(AT.DEFAULTS, **AT.SWITCHES)  # untuned class: defaults
+    ctx = FakeCtx()
+    got = AT.apply(ctx, 10, 10, path=str(p), overrides={"color_compact": "-1", "alpha": 7})
+    assert got["alpha"] == 7 and ctx.calls[0][6] == -1
+    try:
+        AT.apply(ctx, 10, 10, path=str(p), overrides={"nonsense": 1})
+        raise AssertionError("unknown tunable accepted")
+    except KeyError:
+        pass
 
 
 def test_descent_keeps_only_clear_gains():

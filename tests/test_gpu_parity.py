@@ -133,6 +133,30 @@ def test_tuning_does_not_change_labels(tun):
         assert t["async_deg"] == tun["async_deg"]
 
 
+@pytest.mark.parametrize("pair", [1, -1])
+def test_searches_together_and_in_sequence(pair):
+    """The two giant searches run at the same time (the backward one over all
+    active vertices, pivot SCC = F & B) or one after the other (the backward
+    one inside F): same labels, same pivot SCC, graph or direct launches,
+    plain graphs with 32- and 64-bit offsets and a batch of several graphs."""
+    graphs = [G.rmat(15, 16, 2), G.rmat(13, 8, 5, offset_dtype=np.int64), G.planted(40000, 3, giant_frac=0.3),
+              G.planted(30000, 4, giant_frac=0.0, dag_ef=3.0, max_cycle=200)]
+    with Context(1 << 17, 1 << 21) as c:
+        c.set_tuning(pair_searches=pair)
+        assert c.tuning()["pair_searches"] == pair
+        for g in graphs:
+            exact = oracle.tarjan(g)
+            for use_graph in (True, False):
+                labels, st = c.run_csr(g, use_graph=use_graph)
+                assert np.array_equal(labels, exact)
+                vals, counts = np.unique(exact, return_counts=True)
+                assert st["giant_size"] in set(counts.tolist())
+        parts = [G.rmat(11, 8, 7), G.planted(3000, 9, giant_frac=0.5), G.rmat(12, 16, 8)]
+        u, vb = G.disjoint_union(parts)
+        labels, _ = c.run_csr(u, vbase=vb)
+        assert np.array_equal(labels, oracle.tarjan(u))
+
+
 RMAT16 = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "rmat16", "s*.npz")))
 
 
@@ -182,3 +206,87 @@ def test_adjacency_at_unaligned_addresses(ctx):
     fb, bb = torch.from_numpy(csr.fw_beg).cuda(), torch.from_numpy(csr.bw_beg).cuda()
     labels, _ = ctx.run(fb, fa, bb, ba, V=csr.V)
     assert np.array_equal(labels.cpu().numpy(), exact)
+
+
+def _residual_shapes(seed):
+    """A giant ring with chords (the pivot's SCC) and, around it, the shapes
+    the stages after it handle: peel chains into and out of the ring, sink
+    and source 2-cycles, 3-cycles and 3-vertex hubs, a chain of 5-cycles, a
+    vertex between two cycles (a size-1 SCC no trim removes), duplicate
+    edges and self-loops, in shuffled ids."""
+    rng = np.random.default_rng(seed)
+    e = []
+    ring = list(range(3000))
+    e += [(ring[i], ring[(i + 1) % 3000]) for i in range(3000)]
+    e += [(int(a), int(b)) for a, b in rng.integers(0, 3000, (6000, 2))]
+    nxt = 3000
+
+    def new(k):
+        nonlocal nxt
+        ids = list(range(nxt, nxt + k))
+        nxt += k
+        return ids
+
+    for _ in range(20):  # chains out of and into the ring
+        c = new(4)
+        e += [(int(rng.integers(0, 3000)), c[0]), (c[0], c[1]), (c[1], c[2]), (c[2], c[3])]
+        c = new(4)
+        e += [(c[0], c[1]), (c[1], c[2]), (c[2], c[3]), (c[3], int(rng.integers(0, 3000)))]
+    for _ in range(15):  # sink and source 2-cycles hanging off the ring
+        p = new(2)
+        e += [(p[0], p[1]), (p[1], p[0]), (int(rng.integers(0, 3000)), p[0])]
+        p = new(2)
+        e += [(p[0], p[1]), (p[1], p[0]), (p[1], int(rng.integers(0, 3000)))]
+    for _ in range(10):  # 3-cycles and hubs
+        t = new(3)
+        e += [(t[0], t[1]), (t[1], t[2]), (t[2], t[0]), (int(rng.integers(0, 3000)), t[1])]
+        h = new(3)
+        e += [(h[0], h[1]), (h[1], h[0]), (h[0], h[2]), (h[2], h[0]), (h[2], int(rng.integers(0, 3000)))]
+    prev = None
+    for _ in range(12):  # a chain of 5-cycles with chords: mice SCCs
+        c = new(5)
+        e += [(c[i], c[(i + 1) % 5]) for i in range(5)] + [(c[0], c[2])]
+        if prev is not None:
+            e += [(prev[3], c[1]), (prev[4], c[0])]
+        prev = c
+    a, mid, b = new(3), new(1), new(3)  # cycle -> vertex -> cycle
+    e += [(a[0], a[1]), (a[1], a[2]), (a[2], a[0]), (a[1], mid[0]), (mid[0], b[0]),
+          (b[0], b[1]), (b[1], b[2]), (b[2], b[0])]
+    d = new(2)  # a duplicated 2-cycle with a self-loop
+    e += [(d[0], d[1]), (d[0], d[1]), (d[1], d[0]), (d[1], d[1])]
+    perm = rng.permutation(nxt)
+    return G.from_edges(nxt, perm[np.asarray(e, np.int64)])
+
+
+@pytest.mark.parametrize("tiny", [0, -1])
+def test_small_residual_in_one_cta(tiny):
+    """After the giant SCC only a few hundred vertices remain: with the
+    one-CTA path (on by default) and with the stage kernels, the labels, SCC
+    count and size histogram are exact, and both count the same trims."""
+    with Context(1 << 14, 1 << 17) as c:
+        c.set_tuning(tiny_residual=tiny)
+        assert c.tuning()["tiny_residual"] == (1 if tiny == 0 else -1)
+        for seed in (1, 2, 3):
+            g = _residual_shapes(seed)
+            st = check(c, g)
+            assert st["residual"] <= 1024
+            assert st["n_trim2"] > 0 and st["n_trim3"] > 0 and st["n_mice_scc"] > 0
+            for use_graph in (True, False):
+                labels, _ = c.run_csr(g, use_graph=use_graph)
+                assert np.array_equal(labels, oracle.tarjan(g))
+        for seed in range(6):  # random graphs with self-loops and duplicates
+            check(c, G.random_graph(3000, 9000 + 1000 * seed, seed))
+        check(c, G.rmat(12, 8, 4))
+
+
+def test_small_residual_counts_match_stage_kernels():
+    """The one-CTA path records the stage kernels' classification: peeled,
+    trim-2, trim-3 and mice counts equal with the path on and off."""
+    keys = ("scc_count", "giant_size", "n_trim1", "n_trim2", "n_trim3", "n_mice_scc", "n_mice_vertices")
+    got = {}
+    for tiny in (0, -1):
+        with Context(1 << 14, 1 << 17) as c:
+            c.set_tuning(tiny_residual=tiny)
+            _, st = c.run_csr(_residual_shapes(4))
+            got[tiny] = {k: st[k] for k in keys}
+    assert got[0] == got[-1]
