@@ -129,8 +129,10 @@ typedef struct {
                                  intersection): 1 on, -1 off, 0 on for graphs of at most 2^20 vertices */
     int32_t tiny_residual;    /* solve a residual of at most 1024 vertices (and 4096 edges among them per
                                  direction) after the giant SCC in one CTA, skipping the later stage
-                                 kernels: -1 off (0: default, on) */
-    int32_t reserved;
+                                 kernels: 1 on (0: default, off) */
+    int32_t pdl;              /* launch each stage kernel that follows another plain kernel with
+                                 programmatic dependent launch, so its launch overlaps the previous
+                                 kernel's tail: -1 off (0: default, on) */
 } ispan_tuning;
 
 /* NULL restores the defaults; the next run re-captures its CUDA graph. */

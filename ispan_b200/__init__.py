@@ -79,10 +79,10 @@ class Context:
                         1 if on_device else 0)
 
     def set_tuning(self, async_v=0, async_e=0, async_deg=0, bfs_ctas_per_sm=0, color_levels=0,
-                   color_pivots=0, color_compact=0, pair_searches=0, tiny_residual=0) -> None:
+                   color_pivots=0, color_compact=0, pair_searches=0, tiny_residual=0, pdl=0) -> None:
         """Launch tunables (zero = default); see ispan_b200.autotune."""
         t = _lib.Tuning(int(async_v), int(async_e), int(async_deg), int(bfs_ctas_per_sm), int(color_levels),
-                        int(color_pivots), int(color_compact), int(pair_searches), int(tiny_residual), 0)
+                        int(color_pivots), int(color_compact), int(pair_searches), int(tiny_residual), int(pdl))
         check(_lib.lib().ispan_ctx_set_tuning(self._h, C.byref(t)), "ispan_ctx_set_tuning")
 
     def tuning(self) -> dict:

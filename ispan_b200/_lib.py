@@ -63,7 +63,7 @@ class Tuning(C.Structure):
     _fields_ = [("async_v", C.c_int64), ("async_e", C.c_int64), ("async_deg", C.c_int32),
                 ("bfs_ctas_per_sm", C.c_int32), ("color_levels", C.c_int32), ("color_pivots", C.c_int32),
                 ("color_compact", C.c_int32), ("pair_searches", C.c_int32),
-                ("tiny_residual", C.c_int32), ("reserved", C.c_int32)]
+                ("tiny_residual", C.c_int32), ("pdl", C.c_int32)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}

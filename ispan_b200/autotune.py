@@ -33,7 +33,7 @@ TABLE = os.path.join(HERE, "tuning_table.json")
 DEFAULTS = {"alpha": 30, "beta": 200, "gamma": 10, "async_v": 65536, "async_e": 262144, "async_deg": 16,
             "bfs_ctas_per_sm": 0, "color_levels": 32, "color_pivots": 1024}
 # switches that are not searched (0 = the library's default; see ispan_tuning)
-SWITCHES = {"color_compact": 0, "pair_searches": 0, "tiny_residual": 0}
+SWITCHES = {"color_compact": 0, "pair_searches": 0, "tiny_residual": 0, "pdl": 0}
 SPACE = {
     "alpha": [5, 10, 30, 100, 300],
     "beta": [50, 200, 1000, 4000],
@@ -84,7 +84,7 @@ def apply(ctx, V: int, E: int, nseg: int = 1, path: str = TABLE, overrides: dict
             raise KeyError(f"unknown tunable {k!r}")
         p[k] = int(v)
     ctx.set_tuning(p["async_v"], p["async_e"], p["async_deg"], p["bfs_ctas_per_sm"], p["color_levels"],
-                   p["color_pivots"], p["color_compact"], p["pair_searches"], p["tiny_residual"])
+                   p["color_pivots"], p["color_compact"], p["pair_searches"], p["tiny_residual"], p["pdl"])
     return p
 
 

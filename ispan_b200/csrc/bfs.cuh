@@ -494,6 +494,8 @@ __device__ __forceinline__ void rebuild_queue(const Run<OffT> &r, const BfsDir<O
 
 template <typename OffT, int DIR>
 __global__ void __launch_bounds__(kBlock, 2) k_bfs(Run<OffT> r, BfsCtl *ctl) {
+    pdl_wait();  // predecessor done, its writes visible
+    pdl_trigger();
     __shared__ int64_t sh[kWarps];
     constexpr size_t kSm = sizeof(TdSmem) > sizeof(AsyncSmem) ? sizeof(TdSmem) : sizeof(AsyncSmem);
     __shared__ __align__(16) unsigned char smraw[kSm];
@@ -612,6 +614,8 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Run<OffT> r, BfsCtl *ctl) {
 // sum of out-degrees over F and of in-degrees over B.
 template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_reach_degrees(Run<OffT> r) {
+    pdl_wait();  // predecessor done, its writes visible
+    pdl_trigger();
     __shared__ int64_t sh[kWarps];
     const int lane = lane_id();
     const int64_t gw = ((int64_t)blockIdx.x * kBlock + threadIdx.x) >> 5;
@@ -636,6 +640,8 @@ __global__ void __launch_bounds__(kBlock) k_reach_degrees(Run<OffT> r) {
 template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_list_degrees(Run<OffT> r, const int32_t *wl,
                                                          const unsigned long long *n_wl, int slot_n, int slot_deg) {
+    pdl_wait();  // predecessor done, its writes visible
+    pdl_trigger();
     __shared__ int64_t sh[kWarps];
     const int64_t n = (int64_t)*n_wl;
     int64_t d = 0;

@@ -181,6 +181,18 @@ __device__ __forceinline__ int32_t ld_adj(const int32_t *adj, int64_t e) {
 #endif
 }
 __device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
+// Programmatic dependent launch.  The pipeline launches a kernel that
+// follows another plain kernel on its stream with programmatic stream
+// serialization, so its CTAs may be scheduled while the predecessor still
+// runs: every such kernel calls pdl_wait() before its first global memory
+// access (it returns once the predecessor grid has completed and its writes
+// are visible; a no-op in a kernel launched without the attribute), and
+// pdl_trigger() lets the kernel's own successor be scheduled early.  The
+// successor's CTAs are scheduled only after every CTA of this grid has
+// triggered, i.e. started, so waiting CTAs never keep this grid's off the SMs.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 __device__ __forceinline__ unsigned lanemask_lt() {
     unsigned m;
     asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
@@ -261,6 +273,9 @@ __device__ __forceinline__ void st_release_u32(unsigned *p, unsigned v) {
     asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 __device__ __forceinline__ int ld_volatile_int(const int *p) { return *(volatile const int *)p; }
+__device__ __forceinline__ unsigned long long ld_volatile_u64(const unsigned long long *p) {
+    return *(volatile const unsigned long long *)p;
+}
 __device__ __forceinline__ unsigned atom_add_acqrel_u32(unsigned *p, unsigned v) {
     unsigned old;
     asm volatile("atom.add.acq_rel.gpu.global.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");

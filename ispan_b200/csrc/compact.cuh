@@ -54,6 +54,8 @@ struct CmpBufs {
 // (self-loops dropped), and the per scan block sums of the degrees
 template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_cmp_count(Run<OffT> r, Ext<OffT> x, CmpBufs b) {
+    pdl_wait();  // predecessor done, its writes visible
+    pdl_trigger();
     __shared__ int64_t sh[kWarps];
     const int64_t n = (int64_t)__ldcg(x.ctl + K_LARGE);
     if (!cmp_wanted(n, b.V)) return;
@@ -89,6 +91,8 @@ __global__ void __launch_bounds__(kBlock) k_cmp_count(Run<OffT> r, Ext<OffT> x, 
 // thread per block sum, warp scans, then the warp totals); the graph is
 // built only if both directions fit
 __global__ void __launch_bounds__(kScanBlocks) k_cmp_tops(unsigned long long *ctl, CmpBufs b, int nblk) {
+    pdl_wait();  // predecessor done, its writes visible
+    pdl_trigger();
     __shared__ long long wt[2][kScanBlocks / 32];
     const int64_t n = (int64_t)__ldcg(ctl + K_LARGE);
     if (!cmp_wanted(n, b.V)) {
@@ -137,6 +141,8 @@ __global__ void __launch_bounds__(kScanBlocks) k_cmp_tops(unsigned long long *ct
 // over a contiguous sub-range, then a block scan of the thread totals)
 template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_cmp_offsets(Run<OffT> r, Ext<OffT> x, CmpBufs b) {
+    pdl_wait();  // predecessor done, its writes visible
+    pdl_trigger();
     __shared__ int64_t st[kBlock];
     if (!__ldcg(x.ctl + K_CMP_OK)) return;
     const int64_t n = (int64_t)__ldcg(x.ctl + K_LARGE);
@@ -175,6 +181,8 @@ __global__ void __launch_bounds__(kBlock) k_cmp_offsets(Run<OffT> r, Ext<OffT> x
 // compact ids
 template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_cmp_fill(Run<OffT> r, Ext<OffT> x, CmpBufs b) {
+    pdl_wait();  // predecessor done, its writes visible
+    pdl_trigger();
     if (!__ldcg(x.ctl + K_CMP_OK)) return;
     const int64_t n = (int64_t)__ldcg(x.ctl + K_LARGE);
     for (int64_t i = (int64_t)blockIdx.x * kBlock + threadIdx.x; i < n; i += (int64_t)gridDim.x * kBlock) {

@@ -162,8 +162,8 @@ struct ispan_ctx {
     int g_coop_w = 0;           // offset width the coop grids were computed for
 
     // CUDA graph cache
-    cudaGraphExec_t gexec = nullptr;
-    char gkey[256];
+    cudaGraphExec_t gexec[2] = {nullptr, nullptr};  // without / with the stage-time events
+    char gkey[2][256];
     bool graph_broken = false;
     cudaEvent_t ev[kNumEv];
     bool have_ev = false;
@@ -178,6 +178,15 @@ struct ispan_ctx {
 };
 
 static int64_t words_of(int64_t V) { return (V + 31) / 32 + 1; }
+
+// the cached CUDA graphs hold pointers and launch shapes: dropped whenever those change
+static void drop_graphs(ispan_ctx *c) {
+    for (int i = 0; i < 2; ++i)
+        if (c->gexec[i]) {
+            cudaGraphExecDestroy(c->gexec[i]);
+            c->gexec[i] = nullptr;
+        }
+}
 
 static constexpr int64_t kL2WindowMinBytes = 4 << 20;  // status maps smaller than this get no L2 window
 static constexpr int kCtlCounters = 0;                       // kNumCounters
@@ -272,10 +281,7 @@ static int ctx_segments(ispan_ctx *c, int64_t nseg) {
         return ISPAN_ERR_NOMEM;
     }
     c->maxSeg = n;
-    if (c->gexec) {
-        cudaGraphExecDestroy(c->gexec);
-        c->gexec = nullptr;
-    }
+    drop_graphs(c);
     c->vbase_host.clear();
     return ISPAN_OK;
 }
@@ -410,6 +416,23 @@ static void compact_run(const Run<OffT> &r, const Ext<OffT> &x, const CmpBufs &b
     xc.old = b.old;
 }
 
+// A plain launch, with programmatic stream serialization when pdl is set.
+template <typename... P, typename... A>
+static cudaError_t launch_k(bool pdl, void (*k)(P...), int64_t grid, int block, cudaStream_t s, A... args) {
+    cudaLaunchConfig_t cfg;
+    memset(&cfg, 0, sizeof cfg);
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3((unsigned)block);
+    cfg.stream = s;
+    cudaLaunchAttribute at;
+    memset(&at, 0, sizeof at);
+    at.id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at.val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = &at;
+    cfg.numAttrs = pdl ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, k, args...);
+}
+
 template <typename Kern, typename... Args>
 static cudaError_t launch_coop(Kern k, int grid, cudaStream_t s, Args... args) {
     void *ptrs[] = {(void *)&args...};
@@ -441,10 +464,17 @@ static cudaError_t enqueue(ispan_ctx *c, Run<OffT> r, Ext<OffT> x, bool times, b
     cudaError_t e;
     const bool pair = pair_searches(c, r);
     if (pair) r.flags |= kRunPair;
+    // a plain kernel that directly follows another plain kernel on s is
+    // launched for programmatic dependent launch (see pdl_wait); after an
+    // event or a cooperative launch the ordinary stream order applies
+    bool prev_plain = false;
+    const bool pdl_ok = c->tuning.pdl >= 0;
 #define EV(i) \
-    if (times) { e = cudaEventRecordWithFlags(c->ev[i], s, capturing ? cudaEventRecordExternal : 0); if (e) return e; }
+    if (times) { e = cudaEventRecordWithFlags(c->ev[i], s, capturing ? cudaEventRecordExternal : 0); if (e) return e; prev_plain = false; }
 #define LK(...) \
     do { __VA_ARGS__; e = cudaGetLastError(); if (e) return e; } while (0)
+#define PK(kern, grid, block, ...) \
+    do { e = launch_k(pdl_ok && prev_plain, kern, (grid), (block), s, __VA_ARGS__); if (e) return e; prev_plain = true; } while (0)
     EV(0);
     {   // every per-run counter, map and table that starts at zero, in one launch
         ResetDesc rd;
@@ -457,9 +487,9 @@ static cudaError_t enqueue(ispan_ctx *c, Run<OffT> r, Ext<OffT> x, bool times, b
         rd.z[6] = {c->gsize, r.nseg * 8};
         rd.gmin = c->gmin;
         rd.nseg = r.nseg;
-        LK((k_reset<<<std::min<int64_t>(G, 4 * c->nsm), 256, 0, s>>>(rd)));
+        PK((k_reset), std::min<int64_t>(G, 4 * c->nsm), 256, rd);
     }
-    LK((k_trim1_first<OffT><<<G, kBlock, 0, s>>>(r, x)));
+    PK((k_trim1_first<OffT>), G, kBlock, r, x);
     EV(1);
     const int gseed = (int)std::max<int64_t>(1, (r.nseg + 1023) / 1024);
     Run<OffT> rb = r;  // the backward search counts in its own queue and level slots
@@ -475,50 +505,60 @@ static cudaError_t enqueue(ispan_ctx *c, Run<OffT> r, Ext<OffT> x, bool times, b
         rb.qchunk[1] = c->cnt_in;
         rb.P = c->D;
         rb.gsync = c->gsync + kGridSyncWords;
-        LK((k_seed<OffT, 0><<<gseed, 32 * 32, 0, s>>>(r)));
-        LK((k_seed<OffT, 1><<<gseed, 32 * 32, 0, s>>>(rb)));
+        PK((k_seed<OffT, 0>), gseed, 32 * 32, r);
+        PK((k_seed<OffT, 1>), gseed, 32 * 32, rb);
         if ((e = cudaEventRecord(c->ev_fork, s))) return e;
+        prev_plain = false;
         if ((e = cudaStreamWaitEvent(c->stream2, c->ev_fork, 0))) return e;
         if ((e = launch_coop(k_bfs<OffT, 1>, c->g_pair, c->stream2, rb, c->bfsctl))) return e;
+        prev_plain = false;
         if ((e = launch_coop(k_bfs<OffT, 0>, c->g_pair, s, r, c->bfsctl))) return e;
+        prev_plain = false;
         EV(2);
         if ((e = cudaEventRecord(c->ev_join, c->stream2))) return e;
         if ((e = cudaStreamWaitEvent(s, c->ev_join, 0))) return e;
+        prev_plain = false;
     } else {
-        LK((k_seed<OffT, 0><<<gseed, 32 * 32, 0, s>>>(r)));
+        PK((k_seed<OffT, 0>), gseed, 32 * 32, r);
         if ((e = launch_coop(k_bfs<OffT, 0>, c->g_coop[0], s, r, c->bfsctl))) return e;
+        prev_plain = false;
         EV(2);
-        LK((k_seed<OffT, 1><<<gseed, 32 * 32, 0, s>>>(rb)));
+        PK((k_seed<OffT, 1>), gseed, 32 * 32, rb);
         if ((e = launch_coop(k_bfs<OffT, 1>, c->g_coop[1], s, rb, c->bfsctl))) return e;
+        prev_plain = false;
     }
-    if (r.flags & ISPAN_F_EXACT_STATS) LK((k_reach_degrees<OffT><<<G, kBlock, 0, s>>>(r)));
+    if (r.flags & ISPAN_F_EXACT_STATS) PK((k_reach_degrees<OffT>), G, kBlock, r);
     EV(3);
-    LK((k_giant_residual<OffT><<<G, kBlock, 0, s>>>(r, x)));
-    if (r.flags & ISPAN_F_EXACT_STATS) LK((k_list_degrees<OffT><<<G, kBlock, 0, s>>>(r, r.wl[0], x.ctl + K_WL0, -1, C_Q1_XDEG)));
+    PK((k_giant_residual<OffT>), G, kBlock, r, x);
+    if (r.flags & ISPAN_F_EXACT_STATS) PK((k_list_degrees<OffT>), G, kBlock, r, r.wl[0], x.ctl + K_WL0, -1, C_Q1_XDEG);
     EV(4);
-    // a residual of at most kTinyV vertices is solved here in one CTA, and
-    // every stage kernel up to the finalisation then returns at once
-    if (c->tuning.tiny_residual >= 0) LK((k_tiny_residual<OffT><<<1, kBlock, 0, s>>>(r, x)));
+    // on request, a residual of at most kTinyV vertices is solved here in
+    // one CTA, and every stage kernel up to the finalisation then returns at
+    // once (off by default: on R-MAT graphs the residual holds hubs whose
+    // lists one CTA scans slower than the stage kernels' full grids)
+    if (c->tuning.tiny_residual > 0) PK((k_tiny_residual<OffT>), 1, kBlock, r, x);
     if ((e = launch_coop(k_trim1<OffT>, c->g_coop[2], s, r, x, 0, 1, 1))) return e;
-    if (r.flags & ISPAN_F_EXACT_STATS) LK((k_list_degrees<OffT><<<G, kBlock, 0, s>>>(r, r.wl[1], x.ctl + K_WL1, C_Q2_N, C_Q2_XDEG)));
+    prev_plain = false;
+    if (r.flags & ISPAN_F_EXACT_STATS) PK((k_list_degrees<OffT>), G, kBlock, r, r.wl[1], x.ctl + K_WL1, C_Q2_N, C_Q2_XDEG);
     EV(5);
-    LK((k_trim2<OffT><<<G, kBlock, 0, s>>>(r, x, x.cand, x.ctl + K_CAND)));
+    PK((k_trim2<OffT>), G, kBlock, r, x, x.cand, x.ctl + K_CAND);
     EV(6);
-    LK((k_trim3<OffT><<<G, kBlock, 0, s>>>(r, x, x.cand, x.ctl + K_CAND)));
+    PK((k_trim3<OffT>), G, kBlock, r, x, x.cand, x.ctl + K_CAND);
     EV(7);
     // the first peel left its cascade counters and the consumed list count at zero
     if ((e = launch_coop(k_trim1<OffT>, c->g_coop[2], s, r, x, 1, 0, 0))) return e;
+    prev_plain = false;
     EV(8);
-    LK((k_wcc_init<OffT><<<G, kBlock, 0, s>>>(r, x, 0)));
-    LK((k_wcc_hook<OffT><<<G, kBlock, 0, s>>>(r, x, 0, 0)));
-    LK((k_wcc_compress<OffT><<<G, kBlock, 0, s>>>(r, x, 0)));
-    LK((k_wcc_giant<OffT><<<1, kWccRootSamples, 0, s>>>(r, x, 0)));
-    LK((k_wcc_hook<OffT><<<G, kBlock, 0, s>>>(r, x, 0, 1)));
-    LK((k_wcc_flatten<OffT><<<G, kBlock, 0, s>>>(r, x, 0)));
-    LK((k_wcc_alloc<OffT><<<G, kBlock, 0, s>>>(r, x)));
-    LK((k_wcc_scatter<OffT><<<G, kBlock, 0, s>>>(r, x, 0)));
+    PK((k_wcc_init<OffT>), G, kBlock, r, x, 0);
+    PK((k_wcc_hook<OffT>), G, kBlock, r, x, 0, 0);
+    PK((k_wcc_compress<OffT>), G, kBlock, r, x, 0);
+    PK((k_wcc_giant<OffT>), 1, kWccRootSamples, r, x, 0);
+    PK((k_wcc_hook<OffT>), G, kBlock, r, x, 0, 1);
+    PK((k_wcc_flatten<OffT>), G, kBlock, r, x, 0);
+    PK((k_wcc_alloc<OffT>), G, kBlock, r, x);
+    PK((k_wcc_scatter<OffT>), G, kBlock, r, x, 0);
     EV(9);
-    LK((k_local_scc<OffT><<<c->nsm * 6, kLocalThreads, 0, s>>>(r, x)));
+    PK((k_local_scc<OffT>), c->nsm * 6, kLocalThreads, r, x);
     EV(10);
     if (c->tuning.color_compact >= 0 && r.V >= 4 * kCmpMin) {  // (smaller graphs never qualify)
         // the large WCCs' subgraph in dense ids (compact.cuh), then the
@@ -538,21 +578,24 @@ static cudaError_t enqueue(ispan_ctx *c, Run<OffT> r, Ext<OffT> x, bool times, b
         b.cap_e = 2 * (c->maxV + 32);
         b.V = r.V;
         const int nblk = (int)std::max<int64_t>(1, std::min<int64_t>(kScanBlocks, r.V / 4));
-        LK((k_cmp_count<OffT><<<nblk, kBlock, 0, s>>>(r, x, b)));
-        LK((k_cmp_tops<<<1, kScanBlocks, 0, s>>>(x.ctl, b, nblk)));
-        LK((k_cmp_offsets<OffT><<<nblk, kBlock, 0, s>>>(r, x, b)));
-        LK((k_cmp_fill<OffT><<<G, kBlock, 0, s>>>(r, x, b)));
+        PK((k_cmp_count<OffT>), nblk, kBlock, r, x, b);
+        PK((k_cmp_tops), 1, kScanBlocks, x.ctl, b, nblk);
+        PK((k_cmp_offsets<OffT>), nblk, kBlock, r, x, b);
+        PK((k_cmp_fill<OffT>), G, kBlock, r, x, b);
         Run<int32_t> rc;
         Ext<int32_t> xc;
         compact_run(r, x, b, rc, xc);
         if ((e = launch_coop(k_color<int32_t>, c->g_coop[4], s, rc, xc))) return e;
+        prev_plain = false;
     }
     if ((e = launch_coop(k_color<OffT>, c->g_coop[3], s, r, x))) return e;
+    prev_plain = false;
     EV(11);
-    LK((k_finalize<OffT><<<G, kBlock, 0, s>>>(r, x)));
+    PK((k_finalize<OffT>), G, kBlock, r, x);
     EV(12);
 #undef EV
 #undef LK
+#undef PK
     return cudaSuccess;
 }
 
@@ -653,9 +696,10 @@ static int run_t(ispan_ctx *c, int64_t V, int64_t E, int32_t nseg, const OffT *f
         CK(cudaStreamSynchronize(c->stream));
     }
 #endif
-    // stage events are always recorded (they are nodes of the captured graph);
-    // they are read back only when the caller asks for stage times
-    const bool times = (flags & ISPAN_F_STAGE_TIMES) && st;
+    // stage events are recorded (and captured) only when the caller asks for
+    // stage times
+    const bool times = (flags & ISPAN_F_STAGE_TIMES) && st && c->have_ev;
+    const int ev_on = times ? 1 : 0;
     // the window pays only for maps larger than what stays in L2 anyway; on
     // small graphs its attribute calls would cost more than the run's stages
     const bool l2win = !(flags & ISPAN_F_NO_L2_WINDOW) && 6 * r.W * 4 >= kL2WindowMinBytes;
@@ -667,34 +711,38 @@ static int run_t(ispan_ctx *c, int64_t V, int64_t E, int32_t nseg, const OffT *f
                  (long long)E, nseg, (const void *)fwb, (const void *)bwb, (const void *)fwa, (const void *)bwa,
                  (void *)label_dev, r.alpha, r.beta, r.gamma, (void *)c->stream,
                  r.flags & (ISPAN_F_EXACT_STATS | ISPAN_F_NO_L2_WINDOW));
-        if (!c->gexec || strcmp(key, c->gkey) != 0) {
-            if (c->gexec) {
-                cudaGraphExecDestroy(c->gexec);
-                c->gexec = nullptr;
+        // two cached graphs: with the stage-time events (requested times) and
+        // without them, so a run that reads no times pays for no event nodes
+        cudaGraphExec_t &gx = c->gexec[ev_on];
+        char *gk = c->gkey[ev_on];
+        if (!gx || strcmp(key, gk) != 0) {
+            if (gx) {
+                cudaGraphExecDestroy(gx);
+                gx = nullptr;
             }
             cudaGraph_t g = nullptr;
             cudaError_t e = cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal);
             if (e == cudaSuccess) {
-                cudaError_t e2 = enqueue<OffT>(c, r, x, c->have_ev, true);
+                cudaError_t e2 = enqueue<OffT>(c, r, x, ev_on, true);
                 e = cudaStreamEndCapture(c->stream, &g);
                 if (e2 != cudaSuccess) e = e2;
             }
-            if (e == cudaSuccess) e = cudaGraphInstantiate(&c->gexec, g, 0);
+            if (e == cudaSuccess) e = cudaGraphInstantiate(&gx, g, 0);
             if (g) cudaGraphDestroy(g);
             if (e != cudaSuccess) {
                 cudaGetLastError();
                 c->graph_broken = true;  // fall back to direct launches from now on
-                c->gexec = nullptr;
+                gx = nullptr;
                 use_graph = false;
             } else {
-                snprintf(c->gkey, sizeof c->gkey, "%s", key);
+                snprintf(gk, sizeof c->gkey[0], "%s", key);
             }
         }
     }
     if (use_graph) {
-        CK(cudaGraphLaunch(c->gexec, c->stream));
+        CK(cudaGraphLaunch(c->gexec[ev_on], c->stream));
     } else {
-        CK(enqueue<OffT>(c, r, x, c->have_ev, false));
+        CK(enqueue<OffT>(c, r, x, ev_on, false));
     }
     CK(cudaMemcpyAsync(c->h_counters, c->ctlblk, kNumCounters * sizeof(unsigned long long),
                        cudaMemcpyDeviceToHost, c->stream));
@@ -1126,10 +1174,7 @@ int lane_bind(ispan_ctx *c, void *base, size_t bytes, int64_t V, int64_t E, int6
     r.cap = bytes;
     r.used = (size_t)((256 - ((uintptr_t)base & 255)) & 255);
     c->rg = &r;
-    if (c->gexec) {  // the captured graph holds the previous batch's pointers
-        cudaGraphExecDestroy(c->gexec);
-        c->gexec = nullptr;
-    }
+    drop_graphs(c);  // the captured graph holds the previous batch's pointers
     c->vbase_host.clear();
     c->g_coop_w = 0;
     const int rc = ctx_carve(c, V, E, n, V_host);
@@ -1227,7 +1272,7 @@ int ispan_ctx_destroy(ispan_ctx *c) {
     if (!c) return ISPAN_OK;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
-    if (c->gexec) cudaGraphExecDestroy(c->gexec);
+    drop_graphs(c);
     for (void *p : c->owned) cudaFree(p);
     for (void *p : c->seg_owned) cudaFree(p);
     for (void *p : c->csr_owned) cudaFree(p);
@@ -1257,10 +1302,7 @@ int ispan_ctx_set_stream(ispan_ctx *c, void *stream) {
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
     c->stream = (cudaStream_t)stream;
     c->own_stream = false;
-    if (c->gexec) {
-        cudaGraphExecDestroy(c->gexec);
-        c->gexec = nullptr;
-    }
+    drop_graphs(c);
     return ISPAN_OK;
 }
 
@@ -1272,10 +1314,7 @@ int ispan_ctx_set_tuning(ispan_ctx *c, const ispan_tuning *t) {
     std::lock_guard<std::mutex> lock(c->mu);
     c->tuning = t ? *t : ispan_tuning{0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
     c->g_coop_w = 0;  // recompute the persistent grids
-    if (c->gexec) {   // the captured graph holds the old values
-        cudaGraphExecDestroy(c->gexec);
-        c->gexec = nullptr;
-    }
+    drop_graphs(c);   // the captured graph holds the old values
     return ISPAN_OK;
 }
 
@@ -1290,8 +1329,8 @@ int ispan_ctx_get_tuning(ispan_ctx *c, ispan_tuning *t) {
     t->color_pivots = c->tuning.color_pivots > 0 ? c->tuning.color_pivots : kCPivots;
     t->color_compact = c->tuning.color_compact >= 0 ? 1 : -1;
     t->pair_searches = c->tuning.pair_searches;
-    t->tiny_residual = c->tuning.tiny_residual >= 0 ? 1 : -1;
-    t->reserved = 0;
+    t->tiny_residual = c->tuning.tiny_residual > 0 ? 1 : -1;
+    t->pdl = c->tuning.pdl >= 0 ? 1 : -1;
     return ISPAN_OK;
 }
 

@@ -97,6 +97,8 @@ struct ResetDesc {
 };
 
 __global__ void k_reset(ResetDesc d) {
+    pdl_wait();  // predecessor done, its writes visible
+    pdl_trigger();
     const int64_t gt = (int64_t)blockIdx.x * blockDim.x + threadIdx.x, nt = (int64_t)gridDim.x * blockDim.x;
 #pragma unroll 1
     for (int k = 0; k < 7; ++k) {
@@ -139,6 +141,8 @@ __global__ void k_validate(const OffT *fb, const OffT *bb, const int32_t *fa, co
 // overflows on hubs).
 template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_trim1_first(Run<OffT> r, Ext<OffT> x) {
+    pdl_wait();  // predecessor done, its writes visible
+    pdl_trigger();
     __shared__ int64_t sh[kWarps];
     constexpr int U = 4;  // words per warp step: four independent offset loads in flight
     const int lane = lane_id();
@@ -216,6 +220,8 @@ __global__ void __launch_bounds__(kBlock) k_trim1_first(Run<OffT> r, Ext<OffT> x
 // pivot: mark it, queue it at level 0.  Warp per 32 graphs.
 template <typename OffT, int DIR>
 __global__ void k_seed(Run<OffT> r) {
+    pdl_wait();  // predecessor done, its writes visible
+    pdl_trigger();
     const int lane = lane_id();
     int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     int64_t nwp = ((int64_t)gridDim.x * blockDim.x) >> 5;
@@ -250,6 +256,8 @@ __global__ void k_seed(Run<OffT> r) {
 // atomic per CTA reserves its share of the worklist.
 template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_giant_residual(Run<OffT> r, Ext<OffT> x) {
+    pdl_wait();  // predecessor done, its writes visible
+    pdl_trigger();
     __shared__ int64_t sh[kWarps];
     __shared__ int s_scan[kWarps];
     __shared__ unsigned long long s_base;
@@ -363,6 +371,8 @@ __device__ __forceinline__ void count_active(const OffT *beg, const int32_t *adj
 
 template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_trim1(Run<OffT> r, Ext<OffT> x, int in, int out, int cand) {
+    pdl_wait();  // predecessor done, its writes visible
+    pdl_trigger();
     if (__ldcg(x.ctl + K_TINY)) return;  // the residual was solved in one CTA
     __shared__ int64_t sh[kWarps];
     const int64_t gt = (int64_t)blockIdx.x * kBlock + threadIdx.x;
@@ -523,6 +533,8 @@ __device__ __forceinline__ bool claim(Run<OffT> &r, Ext<OffT> &x, int32_t v, int
 template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_trim2(Run<OffT> r, Ext<OffT> x, const int32_t *wl,
                                                   const unsigned long long *n_wl) {
+    pdl_wait();  // predecessor done, its writes visible
+    pdl_trigger();
     if (__ldcg(x.ctl + K_TINY)) return;  // the residual was solved in one CTA
     __shared__ int64_t sh[kWarps];
     const int64_t n = (int64_t)__ldcg(n_wl);
@@ -552,6 +564,8 @@ __global__ void __launch_bounds__(kBlock) k_trim2(Run<OffT> r, Ext<OffT> x, cons
 template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_trim3(Run<OffT> r, Ext<OffT> x, const int32_t *wl,
                                                   const unsigned long long *n_wl) {
+    pdl_wait();  // predecessor done, its writes visible
+    pdl_trigger();
     if (__ldcg(x.ctl + K_TINY)) return;  // the residual was solved in one CTA
     __shared__ int64_t sh[kWarps];
     const int64_t n = (int64_t)__ldcg(n_wl);
@@ -619,6 +633,8 @@ __device__ __forceinline__ int32_t uf_root(const int32_t *parent, int32_t x) {
 
 template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_wcc_init(Run<OffT> r, Ext<OffT> x, int in) {
+    pdl_wait();  // predecessor done, its writes visible
+    pdl_trigger();
     if (__ldcg(x.ctl + K_TINY)) return;  // the residual was solved in one CTA
     const int64_t n = (int64_t)__ldcg(x.ctl + K_WL0 + in);
     for (int64_t i = (int64_t)blockIdx.x * kBlock + threadIdx.x; i < n; i += (int64_t)gridDim.x * kBlock) {
@@ -672,6 +688,8 @@ constexpr int64_t kWccSkipMin = 1 << 14;  // smaller worklists: no sample, every
 
 template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_wcc_hook(Run<OffT> r, Ext<OffT> x, int in, int phase) {
+    pdl_wait();  // predecessor done, its writes visible
+    pdl_trigger();
     if (__ldcg(x.ctl + K_TINY)) return;  // the residual was solved in one CTA
     const int64_t n = (int64_t)__ldcg(x.ctl + K_WL0 + in);
     const bool skip_giant = phase == 1 && __ldcg(x.ctl + K_WCC_GIANT) != 0;
@@ -696,6 +714,8 @@ __global__ void __launch_bounds__(kBlock) k_wcc_hook(Run<OffT> r, Ext<OffT> x, i
 // vertices and records the most frequent one if it holds half the sample
 template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_wcc_compress(Run<OffT> r, Ext<OffT> x, int in) {
+    pdl_wait();  // predecessor done, its writes visible
+    pdl_trigger();
     if (__ldcg(x.ctl + K_TINY)) return;  // the residual was solved in one CTA
     const int64_t n = (int64_t)__ldcg(x.ctl + K_WL0 + in);
     for (int64_t i = (int64_t)blockIdx.x * kBlock + threadIdx.x; i < n; i += (int64_t)gridDim.x * kBlock) {
@@ -706,6 +726,8 @@ __global__ void __launch_bounds__(kBlock) k_wcc_compress(Run<OffT> r, Ext<OffT> 
 
 template <typename OffT>
 __global__ void __launch_bounds__(kWccRootSamples) k_wcc_giant(Run<OffT> r, Ext<OffT> x, int in) {
+    pdl_wait();  // predecessor done, its writes visible
+    pdl_trigger();
     if (__ldcg(x.ctl + K_TINY)) return;  // the residual was solved in one CTA
     __shared__ int32_t roots[kWccRootSamples];
     __shared__ int best, best_n;
@@ -734,6 +756,8 @@ __global__ void __launch_bounds__(kWccRootSamples) k_wcc_giant(Run<OffT> r, Ext<
 // flatten, count members per root, list the roots
 template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_wcc_flatten(Run<OffT> r, Ext<OffT> x, int in) {
+    pdl_wait();  // predecessor done, its writes visible
+    pdl_trigger();
     if (__ldcg(x.ctl + K_TINY)) return;  // the residual was solved in one CTA
     const int64_t n = (int64_t)__ldcg(x.ctl + K_WL0 + in);
     for (int64_t i = (int64_t)blockIdx.x * kBlock + threadIdx.x; i - threadIdx.x < n;
@@ -756,6 +780,8 @@ __global__ void __launch_bounds__(kBlock) k_wcc_flatten(Run<OffT> r, Ext<OffT> x
 // Reserve member space for small WCCs; route the rest to the large path.
 template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_wcc_alloc(Run<OffT> r, Ext<OffT> x) {
+    pdl_wait();  // predecessor done, its writes visible
+    pdl_trigger();
     if (__ldcg(x.ctl + K_TINY)) return;  // the residual was solved in one CTA
     const int64_t n = (int64_t)__ldcg(x.ctl + K_ROOTS);
     for (int64_t i = (int64_t)blockIdx.x * kBlock + threadIdx.x; i - threadIdx.x < n;
@@ -777,6 +803,8 @@ __global__ void __launch_bounds__(kBlock) k_wcc_alloc(Run<OffT> r, Ext<OffT> x) 
 
 template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_wcc_scatter(Run<OffT> r, Ext<OffT> x, int in) {
+    pdl_wait();  // predecessor done, its writes visible
+    pdl_trigger();
     if (__ldcg(x.ctl + K_TINY)) return;  // the residual was solved in one CTA
     const int64_t n = (int64_t)__ldcg(x.ctl + K_WL0 + in);
     for (int64_t i = (int64_t)blockIdx.x * kBlock + threadIdx.x; i - threadIdx.x < n;
@@ -809,6 +837,8 @@ constexpr int kLocalThreads = 256;
 
 template <typename OffT>
 __global__ void __launch_bounds__(kLocalThreads) k_local_scc(Run<OffT> r, Ext<OffT> x) {
+    pdl_wait();  // predecessor done, its writes visible
+    pdl_trigger();
     if (__ldcg(x.ctl + K_TINY)) return;  // the residual was solved in one CTA
     __shared__ int32_t gid[kLocalV];
     __shared__ int32_t loff[kLocalV + 1];
@@ -1089,6 +1119,8 @@ struct ColorSmem {
     int phead, ptail;           // pool entries [phead, ptail); guarded by lock
     int active;                 // warps working (not waiting for pool work); guarded by lock
     int lock;
+    unsigned long long st[4];   // diagnostics of the round (pops, edges, queued, wait ns); see cst
+    long long *cst;             // where they go (null: not recorded)
 };
 
 // CTA spin lock in shared memory, taken by one lane.  Holders keep it for a
@@ -1129,7 +1161,7 @@ __device__ __forceinline__ void cta_unlock(int *l) {
 template <typename OffT, int KIND>
 __device__ __forceinline__ void color_async_round(const Run<OffT> &r, const Ext<OffT> &x, const int32_t *q_in,
                                                   int64_t n_in, int32_t *q_out, unsigned long long *n_out,
-                                                  ColorSmem &sm, long long *cst) {
+                                                  ColorSmem &sm, long long *cst_arg) {
     unsigned long long *cc = reinterpret_cast<unsigned long long *>(r.qe[0]);  // class | colour | flag
     int32_t *rootof = r.aux2;
     const OffT *beg = KIND == 0 ? r.fw_beg : r.bw_beg;
@@ -1145,12 +1177,13 @@ __device__ __forceinline__ void color_async_round(const Run<OffT> &r, const Ext<
         sm.ptail = 0;
         sm.active = kWarps;
         sm.lock = 0;
+        sm.st[0] = sm.st[1] = sm.st[2] = sm.st[3] = 0ull;
+        sm.cst = cst_arg;
     }
     __syncthreads();
     int head = 0, tail = 0;  // ring [head, tail), warp-uniform
     const int cap = 4 * r.color_levels;
     bool capped = false;
-    long long st_pops = 0, st_edges = 0, st_push = 0, st_wait = 0;  // diagnostics (cst set)
     for (int chunk = 0;; ++chunk) {
         if (chunk >= cap) { capped = true; break; }
         int nb = 0;
@@ -1172,7 +1205,7 @@ __device__ __forceinline__ void color_async_round(const Run<OffT> &r, const Ext<
                 if (lane == 0) {
                     bool idle = false;
                     const uint64_t t0 = globaltimer();
-                    if (cst) st_wait -= (long long)t0;
+                    if (sm.cst) atomicAdd(&sm.st[3], 0ull - (unsigned long long)t0);  // diagnostics
                     for (int it = 0;; ++it) {
                         // test without the lock first: waiting warps poll, the lock
                         // stays free for the warps that feed the pool
@@ -1198,12 +1231,14 @@ __device__ __forceinline__ void color_async_round(const Run<OffT> &r, const Ext<
                         }
                         __nanosleep(64);
                     }
-                    if (cst) st_wait += (long long)globaltimer();
+                    if (sm.cst) atomicAdd(&sm.st[3], (unsigned long long)globaltimer());
                 }
                 got = __shfl_sync(kFull, got, 0);
                 if (got == 0) break;  // nothing left in this CTA for this round
                 pb = __shfl_sync(kFull, pb, 0);
                 nb = got;
+                // the pool entries' vertex state was published before them
+                // (block fence on the pushing side); see the push below
                 if (lane < nb) v = sm.pool[(pb + lane) & (kCPool - 1)];
                 __syncwarp();
                 if (lane == 0) cta_unlock(&sm.lock);
@@ -1230,8 +1265,10 @@ __device__ __forceinline__ void color_async_round(const Run<OffT> &r, const Ext<
         }
         const int64_t total = __shfl_sync(kFull, incl, 31);
         base -= incl - deg;  // edge index of the chunk's k-th edge, k in this lane's range: base + k
-        st_pops += nb;
-        st_edges += total;
+        if (sm.cst && lane == 0) {  // diagnostics, in shared memory (no registers held across the loop)
+            atomicAdd(&sm.st[0], (unsigned long long)nb);
+            atomicAdd(&sm.st[1], (unsigned long long)total);
+        }
         for (int64_t k0 = 0; k0 < total; k0 += 64) {
             int32_t w[2], vo[2];
             unsigned long long po[2], pw[2];
@@ -1252,37 +1289,56 @@ __device__ __forceinline__ void color_async_round(const Run<OffT> &r, const Ext<
             }
 #pragma unroll
             for (int u = 0; u < 2; ++u) pw[u] = (w[u] >= 0 && w[u] != vo[u]) ? __ldcg(cc + w[u]) : 0ull;
+            // KIND 0: the first compare-and-swap of both sub-batches in flight
+            // together (they are independent); a failed one retries alone
+            bool pushes[2];
+            if (KIND == 0) {
+                unsigned long long nw[2], seen[2];
+                bool act[2];
 #pragma unroll
-            for (int u = 0; u < 2; ++u) {
-                // the class compare also rejects inactive neighbours (dead class)
-                bool push = w[u] >= 0 && w[u] != vo[u] && (pw[u] >> 32) == (po[u] >> 32);
-                if (push) {
-                    if (KIND == 0) {
+                for (int u = 0; u < 2; ++u) {
+                    // the class compare also rejects inactive neighbours (dead
+                    // class); lower the colour and clear the flag -- the class
+                    // cannot change under a successful swap (it is compared first)
+                    const uint32_t cv = colour_of(po[u]);
+                    act[u] = w[u] >= 0 && w[u] != vo[u] && (pw[u] >> 32) == (po[u] >> 32) && colour_of(pw[u]) > cv;
+                    nw[u] = (po[u] & 0xffffffff00000000ull) | ((unsigned long long)cv << 1);
+                }
+#pragma unroll
+                for (int u = 0; u < 2; ++u) seen[u] = act[u] ? atomicCAS(cc + w[u], pw[u], nw[u]) : pw[u];
+#pragma unroll
+                for (int u = 0; u < 2; ++u) {
+                    bool lowered = act[u] && seen[u] == pw[u];
+                    unsigned long long old = lowered ? pw[u] : seen[u];
+                    if (act[u] && !lowered) {
                         const uint32_t cv = colour_of(po[u]);
-                        // lower the colour and clear the flag; the class cannot
-                        // change under a successful swap (it is compared first)
-                        const unsigned long long nw = (po[u] & 0xffffffff00000000ull) | ((unsigned long long)cv << 1);
-                        unsigned long long old = pw[u];
-                        bool lowered = false;
                         int t = 0;
                         // every failed swap saw a lower colour or a pop's flag
                         for (; t < (1 << 20); ++t) {
                             if ((old >> 32) != (po[u] >> 32) || colour_of(old) <= cv) break;
-                            const unsigned long long seen = atomicCAS(cc + w[u], old, nw);
-                            if (seen == old) { lowered = true; break; }
-                            old = seen;
+                            const unsigned long long sn = atomicCAS(cc + w[u], old, nw[u]);
+                            if (sn == old) { lowered = true; break; }
+                            old = sn;
                         }
                         if (t == (1 << 20)) atomicCAS(r.err, 0, kErrOverflow);
-                        push = lowered && (old & 1ull);  // the flag was set: not queued yet
-                    } else {
-                        push = ((pw[u] ^ po[u]) >> 1) == 0 && !bitv(r.F, w[u]) && set_bit(r.F, w[u]);
-                        if (push) rootof[w[u]] = ro[u];
                     }
+                    pushes[u] = lowered && (old & 1ull);  // the flag was set: not queued yet
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+                bool push;
+                if (KIND == 0) {
+                    push = pushes[u];
+                } else {
+                    push = w[u] >= 0 && w[u] != vo[u] && (pw[u] >> 32) == (po[u] >> 32) &&
+                           ((pw[u] ^ po[u]) >> 1) == 0 && !bitv(r.F, w[u]) && set_bit(r.F, w[u]);
+                    if (push) rootof[w[u]] = ro[u];
                 }
                 const unsigned m = __ballot_sync(kFull, push);
                 if (m) {
                     const int cnt = __popc(m), rank = __popc(m & lt);
-                    st_push += cnt;
+                    if (sm.cst && lane == 0) atomicAdd(&sm.st[2], (unsigned long long)cnt);
                     bool placed = false;
                     // one read, broadcast: the branch below must be warp-uniform
                     const int act = __shfl_sync(kFull, ld_volatile_int(&sm.active), 0);
@@ -1296,6 +1352,7 @@ __device__ __forceinline__ void color_async_round(const Run<OffT> &r, const Ext<
                         pt = __shfl_sync(kFull, pt, 0);
                         if (pt >= 0) {
                             if (push) sm.pool[(pt + rank) & (kCPool - 1)] = w[u];
+                            __threadfence_block();  // the vertex's state before the pool entry, for the taking warp
                             __syncwarp();
                             if (lane == 0) {
                                 sm.ptail = pt + cnt;
@@ -1334,13 +1391,8 @@ __device__ __forceinline__ void color_async_round(const Run<OffT> &r, const Ext<
                 if (VOK((long long)(g + i), 18)) q_out[g + i] = ring[(head + i) & (kCWQ - 1)];
         }
     }
-    if (cst && lane == 0) {
-        atomicAdd((unsigned long long *)cst + 0, (unsigned long long)st_pops);
-        atomicAdd((unsigned long long *)cst + 1, (unsigned long long)st_edges);
-        atomicAdd((unsigned long long *)cst + 2, (unsigned long long)st_push);
-        atomicAdd((unsigned long long *)cst + 3, (unsigned long long)st_wait);
-    }
     __syncthreads();
+    if (sm.cst && threadIdx.x < 4) atomicAdd((unsigned long long *)sm.cst + threadIdx.x, sm.st[threadIdx.x]);
     // the unread rest of the slice (left by warps that reached their chunk
     // cap) and what is left in the pool go back to the grid queue
     const int64_t from = min((int64_t)sm.cursor, s1), rest = s1 - from;
@@ -1384,6 +1436,8 @@ __device__ __forceinline__ int color_async(const Run<OffT> &r, const Ext<OffT> &
 // the pipeline launches both forms and one of them returns at once.
 template <typename OffT>
 __global__ void __launch_bounds__(kBlock, 2) k_color(Run<OffT> r, Ext<OffT> x) {
+    pdl_wait();  // predecessor done, its writes visible
+    pdl_trigger();
     __shared__ int64_t sh[kWarps];
     __shared__ ColorSmem sm;
     if ((__ldcg(x.ctl + K_CMP_OK) != 0) != (x.old != nullptr)) return;
@@ -1497,10 +1551,18 @@ __global__ void __launch_bounds__(kBlock, 2) k_color(Run<OffT> r, Ext<OffT> x) {
             t[2] = npiv;
             t[3] = (long long)globaltimer();
         }
+        // a marked vertex's root is a vertex id (compact ids are smaller
+        // still); anything else is an internal error, recorded, and the
+        // access skipped (the root tables hold V entries)
+        const int64_t idb = r.V;
         for (int64_t i = gt; i < n; i += nt) {  // minimum member id and size per SCC
             int32_t v = L[i];
             if (bitv(r.F, v)) {
                 const int32_t rv = __ldcg(rootof + v);
+                if ((uint64_t)(int64_t)rv >= (uint64_t)idb) {
+                    atomicCAS(r.err, 0, kErrOverflow);
+                    continue;
+                }
                 atomicMin(mn + rv, orig_id(x, v));  // labels are original ids
                 atomicAdd(szc + rv, 1);
             }
@@ -1514,7 +1576,8 @@ __global__ void __launch_bounds__(kBlock, 2) k_color(Run<OffT> r, Ext<OffT> x) {
             if (i < n) {
                 v = L[i];
                 if (bitv(r.F, v)) {
-                    const int32_t rv = __ldcg(rootof + v);
+                    int32_t rv = __ldcg(rootof + v);
+                    if ((uint64_t)(int64_t)rv >= (uint64_t)idb) rv = v;  // recorded above as an error
                     const int32_t ov = orig_id(x, v);
                     r.label[ov] = __ldcg(mn + rv);
                     r.cls[ov] = CLS_MICE;
@@ -1562,6 +1625,8 @@ __global__ void __launch_bounds__(kBlock, 2) k_color(Run<OffT> r, Ext<OffT> x) {
 // here is an internal error.
 template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_finalize(Run<OffT> r, Ext<OffT> x) {
+    pdl_wait();  // predecessor done, its writes visible
+    pdl_trigger();
     constexpr int U = 4;
     const int lane = lane_id();
     const int64_t gw = ((int64_t)blockIdx.x * kBlock + threadIdx.x) >> 5;

@@ -203,6 +203,8 @@ __device__ void tiny_trim23(const Run<OffT> &r, TinySmem &s, int n, int size) {
 
 template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_tiny_residual(Run<OffT> r, Ext<OffT> x) {
+    pdl_wait();  // predecessor done, its writes visible
+    pdl_trigger();
     __shared__ TinySmem s;
     const int t = threadIdx.x;
     const int64_t n64 = (int64_t)__ldcg(x.ctl + K_WL0);

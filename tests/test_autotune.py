@@ -30,7 +30,7 @@ def test_lookup_and_apply(tmp_path):
     got = AT.apply(ctx, 65_536, 955_000, path=str(p))
     assert got["alpha"] == 100 and ctx.calls == [(4096, AT.DEFAULTS["async_e"], AT.DEFAULTS["async_deg"], 1,
                                                   AT.DEFAULTS["color_levels"], AT.DEFAULTS["color_pivots"],
-                                                  0, 0, 0)]
+                                                  0, 0, 0, 0)]
     ctx = FakeCtx()
     assert AT.apply(ctx, 10, 10, path=str(p)) == dict(AT.DEFAULTS, **AT.SWITCHES)  # untuned class: defaults
     ctx = FakeCtx()

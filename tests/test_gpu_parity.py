@@ -98,12 +98,14 @@ def test_batch_union(ctx):
 
 
 def test_stage_times_and_no_graph(ctx):
+    """Runs with and without stage times (two cached graphs: with and without
+    the event nodes) and direct launches, alternating on one context."""
     csr = G.rmat(13, 16, 4)
-    labels, st = ctx.run_csr(csr, stage_times=True)
-    assert np.array_equal(labels, oracle.tarjan(csr))
-    assert st["stage_ms"][3] > 0
-    labels, st = ctx.run_csr(csr, use_graph=False)
-    assert np.array_equal(labels, oracle.tarjan(csr))
+    exact = oracle.tarjan(csr)
+    for times, use_graph in ((True, True), (False, True), (True, True), (False, False), (True, False), (False, True)):
+        labels, st = ctx.run_csr(csr, stage_times=times, use_graph=use_graph)
+        assert np.array_equal(labels, exact)
+        assert (st["stage_ms"][3] > 0) == times
 
 
 def test_reference_codes_report(ctx):
@@ -133,8 +135,8 @@ def test_tuning_does_not_change_labels(tun):
         assert t["async_deg"] == tun["async_deg"]
 
 
-@pytest.mark.parametrize("pair", [1, -1])
-def test_searches_together_and_in_sequence(pair):
+@pytest.mark.parametrize("pair,pdl", [(1, 0), (-1, 0), (1, -1)])
+def test_searches_together_and_in_sequence(pair, pdl):
     """The two giant searches run at the same time (the backward one over all
     active vertices, pivot SCC = F & B) or one after the other (the backward
     one inside F): same labels, same pivot SCC, graph or direct launches,
@@ -142,8 +144,8 @@ def test_searches_together_and_in_sequence(pair):
     graphs = [G.rmat(15, 16, 2), G.rmat(13, 8, 5, offset_dtype=np.int64), G.planted(40000, 3, giant_frac=0.3),
               G.planted(30000, 4, giant_frac=0.0, dag_ef=3.0, max_cycle=200)]
     with Context(1 << 17, 1 << 21) as c:
-        c.set_tuning(pair_searches=pair)
-        assert c.tuning()["pair_searches"] == pair
+        c.set_tuning(pair_searches=pair, pdl=pdl)
+        assert c.tuning()["pair_searches"] == pair and c.tuning()["pdl"] == (1 if pdl == 0 else -1)
         for g in graphs:
             exact = oracle.tarjan(g)
             for use_graph in (True, False):
@@ -258,14 +260,14 @@ def _residual_shapes(seed):
     return G.from_edges(nxt, perm[np.asarray(e, np.int64)])
 
 
-@pytest.mark.parametrize("tiny", [0, -1])
+@pytest.mark.parametrize("tiny", [1, 0])
 def test_small_residual_in_one_cta(tiny):
     """After the giant SCC only a few hundred vertices remain: with the
-    one-CTA path (on by default) and with the stage kernels, the labels, SCC
-    count and size histogram are exact, and both count the same trims."""
+    one-CTA path (on request) and with the stage kernels (default), the
+    labels, SCC count and size histogram are exact."""
     with Context(1 << 14, 1 << 17) as c:
         c.set_tuning(tiny_residual=tiny)
-        assert c.tuning()["tiny_residual"] == (1 if tiny == 0 else -1)
+        assert c.tuning()["tiny_residual"] == (1 if tiny == 1 else -1)
         for seed in (1, 2, 3):
             g = _residual_shapes(seed)
             st = check(c, g)
@@ -284,9 +286,9 @@ def test_small_residual_counts_match_stage_kernels():
     trim-2, trim-3 and mice counts equal with the path on and off."""
     keys = ("scc_count", "giant_size", "n_trim1", "n_trim2", "n_trim3", "n_mice_scc", "n_mice_vertices")
     got = {}
-    for tiny in (0, -1):
+    for tiny in (1, 0):
         with Context(1 << 14, 1 << 17) as c:
             c.set_tuning(tiny_residual=tiny)
             _, st = c.run_csr(_residual_shapes(4))
             got[tiny] = {k: st[k] for k in keys}
-    assert got[0] == got[-1]
+    assert got[1] == got[0]
