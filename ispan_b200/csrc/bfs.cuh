@@ -213,7 +213,6 @@ __device__ __forceinline__ void td_chunk(const Run<OffT> &r, const BfsDir<OffT, 
         dg[k] = 0;
         if (w[k] >= 0) {
             dg[k] = (int32_t)d.xdeg(w[k]);
-            msum_other += d.odeg(w[k]);
             nvis += 1;
             if (dg[k] > 0) { ++n; dsum += dg[k]; } else { w[k] = -1; }  // nothing to expand
         }
@@ -444,7 +443,6 @@ __device__ __forceinline__ void async_round(const Run<OffT> &r, const BfsDir<Off
                         if (!(cand[q] && set_bit(d.Vm, w[q]))) continue;
                         int64_t dg = d.xdeg(w[q]);
                         nvis += 1;
-                        msum_other += d.odeg(w[q]);
                         if (dg == 0) continue;
                         int pos = dg <= r.async_deg ? atomicAdd(&sm.cnt[c ^ 1], 1) : kLQ;
                         if (pos < kLQ) {
@@ -508,11 +506,14 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Run<OffT> r, BfsCtl *ctl) {
     LvlSlot *slots = reinterpret_cast<LvlSlot *>(r.lvl);
     (void)ctl;
 
-    // budget for the alpha rule: unexplored expansion-side edges
-    // (a backward search over A, running beside the forward one, takes the
-    // active set's figures: the forward search's are not known yet)
+    // budget for the alpha rule: unexplored expansion-side edges.  The
+    // backward search takes the in-degree sum over the active set, an upper
+    // bound of the sum over F (the forward search does not sum its reached
+    // vertices' in-degrees: two more random offset loads per vertex);
+    // a backward search running beside the forward one also counts its
+    // candidates over A
     const bool over_a = DIR == 0 || (r.flags & kRunPair);
-    int64_t m_unexpl = (int64_t)(DIR == 0 ? r.counters[C_MU0] : over_a ? r.counters[C_MU0_IN] : r.counters[C_FW_MU]);
+    int64_t m_unexpl = (int64_t)(DIR == 0 ? r.counters[C_MU0] : r.counters[C_MU0_IN]);
     const int64_t n_total = (int64_t)(over_a ? r.counters[C_ACTIVE0] : r.counters[C_FW_SIZE]);
     int level = 0, mode = M_TD;
     bool left_bu = false;  // like the reference, a search never returns to bottom-up
@@ -570,8 +571,6 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Run<OffT> r, BfsCtl *ctl) {
         s.m_other = __ldcg(&slots[s_nx].m_other);
         const int64_t nf = (int64_t)s.nvis;
         total_vis += nf;
-        if (DIR == 0 && blockIdx.x == 0 && tid == 0 && s.m_other)
-            atomicAdd(r.counters + C_FW_MU, s.m_other);
         ++level;
         m_unexpl -= (int64_t)s.m_next;
         const unsigned long long pn = __ldcg(r.qpk + s_nx);

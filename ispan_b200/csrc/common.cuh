@@ -77,7 +77,7 @@ enum Counter {
     C_ACTIVE0 = 0,   // active after trim-1-first
     C_MU0,           // sum of out-degrees of the active vertices
     C_FW_SIZE,       // |F|
-    C_FW_MU,         // sum of in-degrees over F (bottom-up budget of the BW search)
+    C_FW_MU,         // (unused: the backward search budgets with C_MU0_IN)
     C_GIANT,         // |S| over all segments
     C_TRIM1,         // vertices labelled by trim-1 (first pass + peels)
     C_TRIM2,         // vertices in trim-2 pairs

@@ -230,14 +230,12 @@ __global__ void k_seed(Run<OffT> r) {
         unsigned long long key = s < r.nseg ? r.pivot_key[s] : 0ull;
         bool ok = key != 0;
         int64_t p = ok ? (int64_t)(0xffffffffull - (key & 0xffffffffull)) : 0;
-        int64_t dg = 0, other = 0;
+        int64_t dg = 0;
         if (ok) {
             if (DIR == 0) {
                 set_bit(r.F, p);
                 dg = ld_off(r.fw_beg, p + 1) - ld_off(r.fw_beg, p);
-                other = ld_off(r.bw_beg, p + 1) - ld_off(r.bw_beg, p);
                 atomicAdd(r.counters + C_FW_SIZE, 1ull);
-                atomicAdd(r.counters + C_FW_MU, (unsigned long long)other);
             } else {
                 set_bit(r.B, p);
                 dg = ld_off(r.bw_beg, p + 1) - ld_off(r.bw_beg, p);
