@@ -1433,7 +1433,10 @@ __device__ __forceinline__ int color_async(const Run<OffT> &r, const Ext<OffT> &
 // built, or on the compact graph (x.old set, r holding its CSR) if it was;
 // the pipeline launches both forms and one of them returns at once.
 template <typename OffT>
-__global__ void __launch_bounds__(kBlock, 2) k_color(Run<OffT> r, Ext<OffT> x) {
+#ifndef ISPAN_COLOR_MIN_CTAS
+#define ISPAN_COLOR_MIN_CTAS 2  // CTAs per SM the colouring kernel is compiled for (registers: 64 at 2)
+#endif
+__global__ void __launch_bounds__(kBlock, ISPAN_COLOR_MIN_CTAS) k_color(Run<OffT> r, Ext<OffT> x) {
     pdl_wait();  // predecessor done, its writes visible
     pdl_trigger();
     __shared__ int64_t sh[kWarps];
