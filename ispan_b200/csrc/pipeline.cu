@@ -552,7 +552,10 @@ static cudaError_t enqueue(ispan_ctx *c, Run<OffT> r, Ext<OffT> x, bool times, b
     PK((k_wcc_init<OffT>), G, kBlock, r, x, 0);
     PK((k_wcc_hook<OffT>), G, kBlock, r, x, 0, 0);
     PK((k_wcc_compress<OffT>), G, kBlock, r, x, 0);
-    PK((k_wcc_giant<OffT>), 1, kWccRootSamples, r, x, 0);
+    if (r.nseg > 1)
+        PK((k_wcc_giant_seg<OffT>), std::max<int64_t>(1, std::min<int64_t>(G, (r.nseg + kWarps - 1) / kWarps)), kBlock, r, x);
+    else
+        PK((k_wcc_giant<OffT>), 1, kWccRootSamples, r, x, 0);
     PK((k_wcc_hook<OffT>), G, kBlock, r, x, 0, 1);
     PK((k_wcc_flatten<OffT>), G, kBlock, r, x, 0);
     PK((k_wcc_alloc<OffT>), G, kBlock, r, x);

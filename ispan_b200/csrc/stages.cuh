@@ -642,6 +642,10 @@ __global__ void __launch_bounds__(kBlock) k_wcc_init(Run<OffT> r, Ext<OffT> x, i
         r.aux2[v] = -1;    // member base of a small WCC
         r.cnt_out[v] = 0;  // fill cursor
     }
+    // a batch's per-graph giant roots are marked in D (free after the peels)
+    if (r.nseg > 1)
+        for (int64_t w = (int64_t)blockIdx.x * kBlock + threadIdx.x; w < r.W; w += (int64_t)gridDim.x * kBlock)
+            r.D[w] = 0u;
 }
 
 // hook the active neighbours adj[e0, e1) of v (four ids, then their active
@@ -690,7 +694,7 @@ __global__ void __launch_bounds__(kBlock) k_wcc_hook(Run<OffT> r, Ext<OffT> x, i
     pdl_trigger();
     if (__ldcg(x.ctl + K_TINY)) return;  // the residual was solved in one CTA
     const int64_t n = (int64_t)__ldcg(x.ctl + K_WL0 + in);
-    const bool skip_giant = phase == 1 && __ldcg(x.ctl + K_WCC_GIANT) != 0;
+    const bool skip_giant = phase == 1 && (r.nseg > 1 || __ldcg(x.ctl + K_WCC_GIANT) != 0);
     const int32_t g = (int32_t)(__ldcg(x.ctl + K_WCC_GIANT) >> 32);
     for (int64_t i = (int64_t)blockIdx.x * kBlock + threadIdx.x; i < n; i += (int64_t)gridDim.x * kBlock) {
         int32_t v = r.wl[in][i];
@@ -700,9 +704,14 @@ __global__ void __launch_bounds__(kBlock) k_wcc_hook(Run<OffT> r, Ext<OffT> x, i
             hook_range(r.parent, r.A, r.fw_adj, v, e0, es);
         } else if (!skip_giant) {
             hook_range(r.parent, r.A, r.fw_adj, v, es, e1);
-        } else if (__ldcg(r.parent + v) != g) {
-            hook_range(r.parent, r.A, r.fw_adj, v, es, e1);
-            hook_range(r.parent, r.A, r.bw_adj, v, ld_off(r.bw_beg, v), ld_off(r.bw_beg, v + 1));
+        } else {
+            // outside its graph's giant WCC (one graph: the sampled root g;
+            // a batch: roots marked in D by k_wcc_giant_seg), link both ways
+            const int32_t pv = __ldcg(r.parent + v);
+            if (r.nseg > 1 ? !bitc(r.D, pv) : pv != g) {
+                hook_range(r.parent, r.A, r.fw_adj, v, es, e1);
+                hook_range(r.parent, r.A, r.bw_adj, v, ld_off(r.bw_beg, v), ld_off(r.bw_beg, v + 1));
+            }
         }
     }
 }
@@ -749,6 +758,37 @@ __global__ void __launch_bounds__(kWccRootSamples) k_wcc_giant(Run<OffT> r, Ext<
     __syncthreads();
     if (t == 0)
         x.ctl[K_WCC_GIANT] = (ns > 0 && 2 * best_n >= ns) ? (((unsigned long long)(uint32_t)best << 32) | 1ull) : 0ull;
+}
+
+// The same for a batch, per graph: a warp samples 32 evenly spaced vertices
+// of its graph's id range; among the active ones (the residual), a root
+// held by at least half of them, and by at least two, is that graph's giant
+// WCC and is marked in D.  Graphs never share a WCC, so no edge joins two
+// marked components, and phase 1 links every edge with an endpoint outside
+// them from that endpoint, as for one graph.
+template <typename OffT>
+__global__ void __launch_bounds__(kBlock) k_wcc_giant_seg(Run<OffT> r, Ext<OffT> x) {
+    pdl_wait();  // predecessor done, its writes visible
+    pdl_trigger();
+    if (__ldcg(x.ctl + K_TINY)) return;  // the residual was solved in one CTA
+    const int lane = lane_id();
+    const int64_t gw = ((int64_t)blockIdx.x * kBlock + threadIdx.x) >> 5;
+    const int64_t nw = ((int64_t)gridDim.x * kBlock) >> 5;
+    for (int64_t sg = gw; sg < r.nseg; sg += nw) {
+        const int64_t v0 = r.vbase[sg], span = r.vbase[sg + 1] - v0;
+        int32_t root = -1;
+        if (span > 0) {
+            const int64_t v = v0 + (int64_t)lane * span / 32;
+            if ((lane < span || span >= 32) && bitc(r.A, v)) root = __ldcg(r.parent + v);
+        }
+        const unsigned act = __ballot_sync(kFull, root >= 0);
+        const unsigned same = __match_any_sync(kFull, root);
+        const int cnt = root >= 0 ? __popc(same & act) : 0;
+        const int best = __reduce_max_sync(kFull, cnt);
+        // the lowest lane holding the most frequent root decides
+        const unsigned lead = __ballot_sync(kFull, cnt == best && best > 0);
+        if (lane == __ffs(lead) - 1 && best >= 2 && 2 * best >= __popc(act)) set_bit(r.D, root);
+    }
 }
 
 // flatten, count members per root, list the roots
