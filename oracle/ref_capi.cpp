@@ -44,8 +44,8 @@ extern "C" int ispan_ref_run64(int64_t V, int64_t E, int64_t *fw_beg, int64_t *f
                                int64_t *scc_id_out, int quiet)
 #endif
 {
-    static_assert(sizeof(*fw_beg) == sizeof(index_t), "offset width of this build");
-    static_assert(sizeof(*fw_adj) == sizeof(vertex_t), "vertex id width of this build");
+    static_assert(sizeof(*fw_beg) == sizeof(index_t), "offset width of the compiled reference");
+    static_assert(sizeof(*fw_adj) == sizeof(vertex_t), "vertex id width of the compiled reference");
     graph g;
     g.fw_beg_pos = (index_t *)fw_beg;
     g.fw_csr = (vertex_t *)fw_adj;

@@ -148,11 +148,13 @@ def test_searches_together_and_in_sequence(pair, pdl):
         assert c.tuning()["pair_searches"] == pair and c.tuning()["pdl"] == (1 if pdl == 0 else -1)
         for g in graphs:
             exact = oracle.tarjan(g)
-            for use_graph in (True, False):
-                labels, st = c.run_csr(g, use_graph=use_graph)
+            for use_graph, extra in ((True, {}), (False, {}), (True, {"exact_stats": True, "stage_times": True})):
+                labels, st = c.run_csr(g, use_graph=use_graph, **extra)
                 assert np.array_equal(labels, exact)
                 vals, counts = np.unique(exact, return_counts=True)
                 assert st["giant_size"] in set(counts.tolist())
+                if extra:  # the statistics runs: degree sums of the reached sets, stage times
+                    assert st["fw_edges"] >= 0 and st["bw_edges"] >= 0 and st["stage_ms"][3] > 0
         parts = [G.rmat(11, 8, 7), G.planted(3000, 9, giant_frac=0.5), G.rmat(12, 16, 8)]
         u, vb = G.disjoint_union(parts)
         labels, _ = c.run_csr(u, vbase=vb)
