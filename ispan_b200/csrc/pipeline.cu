@@ -854,6 +854,8 @@ static int check_csr(const ispan_csr *g) {
 }
 
 // host offsets are validated before upload: monotone, 0..E
+// host offsets of a graph to be packed: monotone from 0 to E (the pack
+// kernels index the adjacency by them)
 static int check_host_offsets(const ispan_csr *g) {
     for (int k = 0; k < 2; ++k) {
         const void *b = k ? g->bw_beg : g->fw_beg;
@@ -923,9 +925,12 @@ static int run_locked(ispan_ctx *c, const ispan_csr *g, int32_t nseg, const int6
     const void *fwb = g->fw_beg, *bwb = g->bw_beg;
     const int32_t *fwa = g->fw_adj, *bwa = g->bw_adj;
     if (!g->on_device) {
-        if ((rc = check_host_offsets(g))) return rc;
+        // the copies' sizes come from V and E alone; the offsets (monotone,
+        // from 0 to E) and the ids of host input are checked on the device,
+        // before any stage reads them (a serial host scan of the offsets
+        // cost more than the upload itself on large graphs)
         if ((rc = upload(c, g))) return rc;
-        c->validate_next = true;  // adjacency ids of host input are checked on the device
+        c->validate_next = true;
         fwb = c->up_fw_beg;
         bwb = c->up_bw_beg;
         fwa = c->up_fw_adj;

@@ -77,6 +77,27 @@ def test_edge_cases(ctx):
     check(ctx, G.toy())
 
 
+def test_malformed_host_input_is_refused(ctx):
+    """Host CSRs are checked on the device before any stage runs: offsets
+    that fall, do not start at 0 or do not end at E, and ids outside [0, V),
+    are refused with ISPAN_ERR_ARG; the context then runs a good graph."""
+    from ispan_b200 import IspanError
+    good = G.rmat(10, 8, 3)
+    bad = []
+    fb = good.fw_beg.copy(); fb[5], fb[6] = fb[6], fb[5] - 1            # falling offsets
+    bad.append(G.CSR(good.V, good.E, fb, good.fw_adj, good.bw_beg, good.bw_adj))
+    bb = good.bw_beg.copy(); bb[-1] -= 1                                 # does not end at E
+    bad.append(G.CSR(good.V, good.E, good.fw_beg, good.fw_adj, bb, good.bw_adj))
+    fa = good.fw_adj.copy(); fa[7] = good.V                              # id out of range
+    bad.append(G.CSR(good.V, good.E, good.fw_beg, fa, good.bw_beg, good.bw_adj))
+    for csr in bad:
+        with pytest.raises(IspanError) as e:
+            ctx.run_csr(csr)
+        assert e.value.code == -1  # ISPAN_ERR_ARG
+    labels, _ = ctx.run_csr(good)
+    assert np.array_equal(labels, oracle.tarjan(good))
+
+
 def test_device_input_and_repeat(ctx):
     import torch
     csr = G.rmat(14, 16, 9, offset_dtype=np.int64)
