@@ -854,22 +854,6 @@ static int check_csr(const ispan_csr *g) {
 }
 
 // host offsets are validated before upload: monotone, 0..E
-// host offsets of a graph to be packed: monotone from 0 to E (the pack
-// kernels index the adjacency by them)
-static int check_host_offsets(const ispan_csr *g) {
-    for (int k = 0; k < 2; ++k) {
-        const void *b = k ? g->bw_beg : g->fw_beg;
-        int64_t prev = 0;
-        for (int64_t i = 0; i <= g->V; ++i) {
-            int64_t x = g->offset_bytes == 4 ? ((const int32_t *)b)[i] : ((const int64_t *)b)[i];
-            if ((i == 0 && x != 0) || x < prev) return ISPAN_ERR_ARG;
-            prev = x;
-        }
-        if (prev != g->E) return ISPAN_ERR_ARG;
-    }
-    return ISPAN_OK;
-}
-
 static int upload(ispan_ctx *c, const ispan_csr *g) {
     size_t ob = (size_t)g->offset_bytes;
     if (c->up_V < g->V || c->up_E < g->E || c->up_fw_beg == nullptr) {
@@ -1022,11 +1006,9 @@ static int pack_graphs(ispan_ctx *c, const ispan_csr *gs, int32_t n) {
         Et += gs[i].E;
     }
     if (Vt > c->maxV || Et > c->maxE) return ISPAN_ERR_CAPACITY;
-    for (int32_t i = 0; i < n; ++i)
-        if (!gs[i].on_device) {
-            int rc = check_host_offsets(&gs[i]);
-            if (rc) return rc;
-        }
+    // host graphs' offsets are checked on the device by k_pack_offsets, like
+    // the device graphs' (the adjacency is packed by edge slot, so no access
+    // depends on an offset before the check)
     int rc = pk_reserve(c, n);
     if (rc) return rc;
     cudaStream_t s = c->stream;

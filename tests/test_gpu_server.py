@@ -73,6 +73,15 @@ def test_run_graphs_rejects_bad_graph(ctx):
     off[3] = off[4] + 1  # offsets decrease from vertex 3 to 4
     with pytest.raises(IspanError):
         ctx.run_graphs([(torch.from_numpy(off).cuda(), fa, bb, ba)])
+    # host graphs are checked on the device the same way: falling offsets,
+    # offsets that do not end at E, ids out of range
+    end = g.bw_beg.copy()
+    end[-1] -= 1
+    for host in ((off, g.fw_adj, g.bw_beg, g.bw_adj), (g.fw_beg, g.fw_adj, end, g.bw_adj),
+                 (g.fw_beg, bad_adj, g.bw_beg, g.bw_adj)):
+        with pytest.raises(IspanError) as e:
+            ctx.run_graphs([host, (G.toy().fw_beg, G.toy().fw_adj, G.toy().bw_beg, G.toy().bw_adj)])
+        assert e.value.code == -1
     # the context still works afterwards
     labels, _ = ctx.run_graphs([_dev(G.toy())])
     assert np.array_equal(labels[0].cpu().numpy(), oracle.tarjan(G.toy()))
