@@ -333,11 +333,14 @@ def cpu_baseline_social(g, args):
 
 
 def e2e_plain(ctx, g, stream, steps, tun, ws):
-    """End to end through the public API: pinned host CSR uploaded every step,
-    labels copied back.  Frees the generator's device arrays first (the
-    upload buffers take their place)."""
+    """End to end through the public API: the pinned host graph uploaded every
+    step, labels copied back; timed with the forward CSR alone (the library
+    builds the reverse on the device, inside the step) and with both CSRs,
+    the record chosen by e2e_pick.  Frees the generator's device arrays first
+    (the upload buffers take their place)."""
     import torch
-    h2d = 2 * (g.V + 1) * 8 + 2 * g.E * 4
+    h2d_fw = (g.V + 1) * 8 + g.E * 4
+    h2d = 2 * h2d_fw
     if host_mem_available() < 1.25 * h2d:
         return {"value": None, "unit": "GTEPS", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": g.V * 4,
                 "unavailable": f"host memory: {host_mem_available() / 1e9:.0f} GB available, "
@@ -347,19 +350,36 @@ def e2e_plain(ctx, g, stream, steps, tun, ws):
     np_args = [t.numpy() for t in (hfb, hfa, hbb, hba)]
     g.free()
     torch.cuda.empty_cache()
-    ctx.run(*np_args, V=g.V, labels_out=hlab.numpy(), **tun)  # warm (allocates the upload buffers)
-    barrier(ws)
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(steps):
-        ctx.run(*np_args, V=g.V, labels_out=hlab.numpy(), **tun)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    ms = max_over_ranks(e0.elapsed_time(e1), ws) / steps
+
+    def timed(args):
+        ctx.run(*args, V=g.V, labels_out=hlab.numpy(), **tun)  # warm (allocates the upload buffers)
+        barrier(ws)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            ctx.run(*args, V=g.V, labels_out=hlab.numpy(), **tun)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return max_over_ranks(e0.elapsed_time(e1), ws) / steps
+
+    ms_fw = timed(np_args[:2] + [None, None])
+    ms_both = timed(np_args)
     del np_args, hfb, hfa, hbb, hba, hlab
-    return {"value": ws * g.E / (ms / 1e3) / 1e9, "unit": "GTEPS", "ms_per_step": ms,
-            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": g.V * 4}
+    rec = lambda ms, h: {"value": ws * g.E / (ms / 1e3) / 1e9, "unit": "GTEPS", "ms_per_step": ms,  # noqa: E731
+                         "h2d_bytes_per_step": h, "d2h_bytes_per_step": g.V * 4}
+    return e2e_pick(g.E, rec(ms_fw, h2d_fw), rec(ms_both, h2d))
+
+
+def e2e_pick(E, fw, both):
+    """The end-to-end record: below 2^31 edges the forward CSR alone is sent
+    (its reverse is sorted on the device, faster than copying it); larger
+    graphs send both directions (their reverse would be placed by atomics,
+    slower than the copy).  The other form is kept as a sub-record."""
+    if E < 2**31 - 1:
+        return dict(fw, input="the forward CSR from pinned host memory; the reverse CSR is built on the device "
+                              "inside the step", both_directions=both)
+    return dict(both, input="both CSRs from pinned host memory", forward_only=fw)
 
 
 def timed_runs(run, stream, steps, warmup, ws):
@@ -469,7 +489,7 @@ def bench_rmat16(args):
     ctx.set_stream(stream)
     if args.tuning:
         ctx.set_tuning(**{k: int(v) for k, v in args.tuning.items()})
-    per, cpu_ms, e2e_ms, st_last = [], [], [], None
+    per, cpu_ms, e2e_ms, e2e_ms2, st_last = [], [], [], [], None
     mism_oracle = mism_ref = n_fixtures = 0
     roofs = []
     clk = None
@@ -502,16 +522,17 @@ def bench_rmat16(args):
         pin = [torch.from_numpy(a).pin_memory() for a in (csr.fw_beg, csr.fw_adj, csr.bw_beg, csr.bw_adj)]
         hl = torch.empty(csr.V, dtype=torch.int32, pin_memory=True)
         host = [p.numpy() for p in pin]
-        for _ in range(args.warmup):
-            ctx.run(*host, V=csr.V, labels_out=hl.numpy())
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(args.small_steps):
-            ctx.run(*host, V=csr.V, labels_out=hl.numpy())
-        e1.record(stream)
-        torch.cuda.synchronize()
-        e2e_ms.append(e0.elapsed_time(e1) / args.small_steps)
+        for k, args_k in enumerate((host[:2] + [None, None], host)):  # forward CSR only; both directions
+            for _ in range(args.warmup):
+                ctx.run(*args_k, V=csr.V, labels_out=hl.numpy())
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(args.small_steps):
+                ctx.run(*args_k, V=csr.V, labels_out=hl.numpy())
+            e1.record(stream)
+            torch.cuda.synchronize()
+            (e2e_ms if k == 0 else e2e_ms2).append(e0.elapsed_time(e1) / args.small_steps)
         if not args.no_cpu_baseline:
             try:
                 cpu_ms.append(statistics.mean(reference_timing_host(csr, 10, 2)))
@@ -538,9 +559,13 @@ def bench_rmat16(args):
         "metric": "SCC GTEPS", "value": gteps, "unit": "GTEPS", "ms_per_step": ms_mean, "steps": args.small_steps,
         "warmup": args.warmup, "mean_edges": E_mean, "per_seed": per,
         "roofline": roof, "cpu_baseline": cpu,
-        "e2e": {"value": statistics.mean(p["E"] / (e / 1e3) / 1e9 for p, e in zip(per, e2e_ms)), "unit": "GTEPS",
-                "ms_per_step": statistics.mean(e2e_ms), "h2d_bytes_per_step": int(2 * 4 * (65537 + E_mean)),
-                "d2h_bytes_per_step": 65536 * 4},
+        "e2e": e2e_pick(E_mean, {
+            "value": statistics.mean(p["E"] / (e / 1e3) / 1e9 for p, e in zip(per, e2e_ms)), "unit": "GTEPS",
+            "ms_per_step": statistics.mean(e2e_ms), "h2d_bytes_per_step": int(4 * (65537 + E_mean)),
+            "d2h_bytes_per_step": 65536 * 4}, {
+            "value": statistics.mean(p["E"] / (e / 1e3) / 1e9 for p, e in zip(per, e2e_ms2)), "unit": "GTEPS",
+            "ms_per_step": statistics.mean(e2e_ms2), "h2d_bytes_per_step": int(2 * 4 * (65537 + E_mean)),
+            "d2h_bytes_per_step": 65536 * 4}),
         "labels_vs_oracle_mismatches": mism_oracle, "labels_vs_reference_fixture_mismatches": mism_ref,
         "reference_fixtures_checked": n_fixtures,
         "stage_ms": stage_summary(mean_stage_ms([st_last])), "clocks": clk,
@@ -758,8 +783,10 @@ def bench_batch(args, ws, rank, local):
                    "sample": f"unavailable: {str(e).splitlines()[0][:200]}"}
     del hosts
     # end to end: the union from pinned host memory through the batched call
+    # (the forward CSR, its reverse built on the device; and both directions)
     e2e = None
-    h2d = 2 * (g.V + 1) * 8 + 2 * g.E * 4
+    h2d_fw = (g.V + 1) * 8 + g.E * 4
+    h2d = 2 * h2d_fw
     if args.e2e_steps > 0 and host_mem_available() < 1.25 * h2d:
         e2e = {"value": None, "unit": "graphs/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": g.V * 4,
                "unavailable": f"host memory: {host_mem_available() / 1e9:.0f} GB available"}
@@ -769,17 +796,23 @@ def bench_batch(args, ws, rank, local):
         np_args = [t.numpy() for t in (hfb, hfa, hbb, hba)]
         g.free()
         torch.cuda.empty_cache()
-        ctx.run(*np_args, V=g.V, labels_out=hlab.numpy(), vbase=vb)  # warm (upload buffers)
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(args.e2e_steps):
-            ctx.run(*np_args, V=g.V, labels_out=hlab.numpy(), vbase=vb)
-        e1.record(stream)
-        torch.cuda.synchronize()
-        ems = max_over_ranks(e0.elapsed_time(e1), ws) / args.e2e_steps
-        e2e = {"value": ws * nseg / (ems / 1e3), "unit": "graphs/s", "ms_per_step": ems,
-               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": g.V * 4}
+
+        def timed(a):
+            ctx.run(*a, V=g.V, labels_out=hlab.numpy(), vbase=vb)  # warm (upload buffers)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(args.e2e_steps):
+                ctx.run(*a, V=g.V, labels_out=hlab.numpy(), vbase=vb)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            return max_over_ranks(e0.elapsed_time(e1), ws) / args.e2e_steps
+
+        ems_fw = timed(np_args[:2] + [None, None])
+        ems_both = timed(np_args)
+        rec = lambda ms, h: {"value": ws * nseg / (ms / 1e3), "unit": "graphs/s", "ms_per_step": ms,  # noqa: E731
+                             "h2d_bytes_per_step": h, "d2h_bytes_per_step": g.V * 4}
+        e2e = e2e_pick(g.E, rec(ems_fw, h2d_fw), rec(ems_both, h2d))
         del np_args, hfb, hfa, hbb, hba, hlab
     ctx.close()
     if plain is not None:

@@ -31,7 +31,9 @@ REFERENCE_DEFAULTS = dict(alpha=30, beta=200, gamma=10, theta=0.1)  # src/bash_o
 
 
 def _ptr(a) -> int:
-    """Data pointer of a numpy array or a torch tensor."""
+    """Data pointer of a numpy array or a torch tensor (0 for None)."""
+    if a is None:
+        return 0
     if hasattr(a, "data_ptr"):
         return a.data_ptr()
     return a.ctypes.data
@@ -90,14 +92,19 @@ class Context:
         check(_lib.lib().ispan_ctx_get_tuning(self._h, C.byref(t)), "ispan_ctx_get_tuning")
         return t.as_dict()
 
-    def run(self, fw_beg, fw_adj, bw_beg, bw_adj, V: int | None = None, labels_out=None,
+    def run(self, fw_beg, fw_adj, bw_beg=None, bw_adj=None, V: int | None = None, labels_out=None,
             vbase=None, alpha=30, beta=200, gamma=10, theta=0.1, stage_times=False, use_graph=True,
-            histogram=False, exact_stats=False, validate=False):
+            histogram=False, exact_stats=False, validate=False, reverse_atomic=False):
         """Detect SCCs.  Arrays are numpy (host) or torch CUDA tensors (device);
         offsets int32 or int64, ids int32.  Returns (labels, stats): labels[V]
         int32 canonical min-id labels, a numpy array for host input or the
         given/new CUDA tensor for device input.  ``vbase`` (numpy int64,
-        nseg+1 entries) runs a disjoint union of graphs as a batch."""
+        nseg+1 entries) runs a disjoint union of graphs as a batch.  With
+        ``bw_beg`` and ``bw_adj`` both None, only the forward CSR is given
+        (and, for host input, copied): the reverse is built on the device,
+        by a sort or, with ``reverse_atomic``, by atomics (no scratch)."""
+        if (bw_beg is None) != (bw_adj is None):
+            raise ValueError("give both reverse arrays or neither")
         on_dev = hasattr(fw_beg, "is_cuda") and fw_beg.is_cuda
         if V is None:
             V = (fw_beg.numel() if hasattr(fw_beg, "numel") else len(fw_beg)) - 1
@@ -115,6 +122,8 @@ class Context:
             flags |= _lib.F_EXACT_STATS
         if validate:
             flags |= _lib.F_VALIDATE
+        if reverse_atomic:
+            flags |= _lib.F_REVERSE_ATOMIC
         if on_dev:
             import torch
             if labels_out is None:

@@ -23,6 +23,7 @@ F_STAGE_TIMES = 4
 F_NO_L2_WINDOW = 8
 F_VALIDATE = 16
 F_EXACT_STATS = 32
+F_REVERSE_ATOMIC = 64
 NOALLOC_MAX_V = 65536
 
 

@@ -21,11 +21,11 @@ FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--extended-lambda", "-Xcompiler", "-
          "-shared", "-I" + os.path.join(ROOT, "include")]
 
 TARGETS = {
-    "libispan_b200.so": (["pipeline.cu", "noalloc.cu", "server.cu", "condense.cu", "shard.cu"], ["common.cuh", "bfs.cuh", "stages.cuh", "pack.cuh", "compact.cuh", "tiny.cuh", "lane.h"], []),
+    "libispan_b200.so": (["pipeline.cu", "noalloc.cu", "server.cu", "condense.cu", "shard.cu"], ["common.cuh", "bfs.cuh", "stages.cuh", "pack.cuh", "compact.cuh", "tiny.cuh", "transpose.cuh", "lane.h"], []),
     "libispan_gen.so": (["gen.cu"], [], []),
 }
 # self-checking variant: range checks on every index, first violation reported
-CHECKED = {"libispan_b200_checked.so": (["pipeline.cu", "noalloc.cu", "server.cu", "condense.cu", "shard.cu"], ["common.cuh", "bfs.cuh", "stages.cuh", "pack.cuh", "compact.cuh", "tiny.cuh", "lane.h"],
+CHECKED = {"libispan_b200_checked.so": (["pipeline.cu", "noalloc.cu", "server.cu", "condense.cu", "shard.cu"], ["common.cuh", "bfs.cuh", "stages.cuh", "pack.cuh", "compact.cuh", "tiny.cuh", "transpose.cuh", "lane.h"],
                                         ["-DISPAN_CHECKED"])}
 
 

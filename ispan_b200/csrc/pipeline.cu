@@ -23,8 +23,12 @@
 #include <mutex>
 #include <vector>
 
+#include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
+
 #include "bfs.cuh"
 #include "pack.cuh"
+#include "transpose.cuh"
 #include "compact.cuh"
 #include "tiny.cuh"
 #include "lane.h"
@@ -82,6 +86,7 @@ __global__ void k_barrier_probe(unsigned *gs, int *err, uint64_t limit_ns) {
 }
 
 constexpr int kNumEv = 13;  // stage boundaries recorded per run
+constexpr int kUpChunks = 8;  // forward adjacency copied in chunks, each counted as it lands
 
 }  // namespace
 
@@ -140,10 +145,22 @@ struct ispan_ctx {
     unsigned long long *pivot_key = nullptr, *gsize = nullptr;
     int32_t *gmin = nullptr;
 
-    // uploaded CSR (host input)
+    // uploaded CSR (host input), and the reverse CSR built on the device
+    // for input that gives the forward direction only
     void *up_fw_beg = nullptr, *up_bw_beg = nullptr;
     int32_t *up_fw_adj = nullptr, *up_bw_adj = nullptr;
     int64_t up_V = -1, up_E = -1;
+    cudaEvent_t ev_up[kUpChunks] = {};  // forward adjacency chunk k copied
+    void *scan_tmp = nullptr;           // the reverse offsets' scan
+    size_t scan_tmp_bytes = 0;
+    // the reverse lists by a radix sort of (id, source) pairs: keys, their
+    // alternate, the sources' alternate, and the sort's temporary storage
+    int32_t *rv_k0 = nullptr, *rv_k1 = nullptr, *rv_v = nullptr;
+    void *rv_tmp = nullptr;
+    size_t rv_tmp_bytes = 0;
+    int64_t rv_E = -1;
+    bool rv_failed = false;  // the scratch did not fit: placement by atomics
+    std::vector<void *> rv_owned;
 
     // host staging
     unsigned long long *h_counters = nullptr;  // pinned
@@ -843,38 +860,157 @@ static int run_t(ispan_ctx *c, int64_t V, int64_t E, int32_t nseg, const OffT *f
     return ISPAN_OK;
 }
 
-static int check_csr(const ispan_csr *g) {
+// a CSR that gives the forward direction only (bw_beg and bw_adj both NULL):
+// the run builds the reverse on the device
+static bool fw_only(const ispan_csr *g) { return g && !g->bw_beg && !g->bw_adj; }
+
+static int check_csr(const ispan_csr *g, bool allow_fw_only = false) {
     if (!g || g->V < 0 || g->E < 0) return ISPAN_ERR_ARG;
     if (g->offset_bytes != 4 && g->offset_bytes != 8) return ISPAN_ERR_ARG;
     if (g->offset_bytes == 4 && g->E > INT32_MAX) return ISPAN_ERR_ARG;
     if (g->V >= INT32_MAX) return ISPAN_ERR_ARG;
-    if (g->V > 0 && (!g->fw_beg || !g->bw_beg)) return ISPAN_ERR_ARG;
-    if (g->E > 0 && (!g->fw_adj || !g->bw_adj)) return ISPAN_ERR_ARG;
+    const bool rev = !(allow_fw_only && fw_only(g));
+    if (g->V > 0 && (!g->fw_beg || (rev && !g->bw_beg))) return ISPAN_ERR_ARG;
+    if (g->E > 0 && (!g->fw_adj || (rev && !g->bw_adj))) return ISPAN_ERR_ARG;
     return ISPAN_OK;
 }
 
-// host offsets are validated before upload: monotone, 0..E
-static int upload(ispan_ctx *c, const ispan_csr *g) {
-    size_t ob = (size_t)g->offset_bytes;
-    if (c->up_V < g->V || c->up_E < g->E || c->up_fw_beg == nullptr) {
-        for (void *p : c->csr_owned) cudaFree(p);
-        c->csr_owned.clear();
-        int rc = 0;
-        char *a = nullptr, *b = nullptr;
-        rc |= dalloc(&a, (size_t)(g->V + 1) * 8, c->csr_owned);
-        rc |= dalloc(&b, (size_t)(g->V + 1) * 8, c->csr_owned);
-        rc |= dalloc(&c->up_fw_adj, (size_t)g->E, c->csr_owned);
-        rc |= dalloc(&c->up_bw_adj, (size_t)g->E, c->csr_owned);
-        if (rc) {
-            c->up_V = c->up_E = -1;
-            c->up_fw_beg = nullptr;
-            return ISPAN_ERR_NOMEM;
-        }
-        c->up_fw_beg = a;
-        c->up_bw_beg = b;
-        c->up_V = g->V;
-        c->up_E = g->E;
+// scratch of the sorted reverse lists for E edges (3 E ids and the sort's
+// storage, kept for later runs); false if it does not fit
+static bool ensure_rev_sort(ispan_ctx *c, int64_t E) {
+    if (!c->rv_failed && c->rv_E >= E) return true;
+    if (c->rv_failed && E >= c->rv_E) return false;
+    for (void *p : c->rv_owned) cudaFree(p);
+    c->rv_owned.clear();
+    c->rv_E = -1;
+    size_t tb = 0;
+    cub::DoubleBuffer<int32_t> k(nullptr, nullptr), v(nullptr, nullptr);
+    bool ok = cub::DeviceRadixSort::SortPairs(nullptr, tb, k, v, (int)E, 0, 32, c->stream) == cudaSuccess;
+    ok = ok && dalloc(&c->rv_k0, (size_t)E, c->rv_owned) == 0 && dalloc(&c->rv_k1, (size_t)E, c->rv_owned) == 0 &&
+         dalloc(&c->rv_v, (size_t)E, c->rv_owned) == 0 && dalloc((char **)&c->rv_tmp, tb, c->rv_owned) == 0;
+    if (!ok) {
+        for (void *p : c->rv_owned) cudaFree(p);
+        c->rv_owned.clear();
+        cudaGetLastError();  // a failed allocation is not an error of the run
+        c->rv_failed = true;
+        c->rv_E = E;  // this size (and larger) takes the atomic placement
+        return false;
     }
+    c->rv_tmp_bytes = tb;
+    c->rv_E = E;
+    c->rv_failed = false;
+    return true;
+}
+
+// The reverse CSR (X = reverse offsets, ba = reverse adjacency) of the
+// forward CSR (fb, fa) on the device.  With `host` set, fb and fa are host
+// arrays: the offsets and then the adjacency, in kUpChunks chunks, are
+// copied into dfb/dfa on c->stream, and each chunk's in-degrees are counted
+// on c->stream2 as soon as it has landed, so counting overlaps the copy.
+template <typename OffT>
+static int build_reverse(ispan_ctx *c, int64_t V, int64_t E, const OffT *fb, const int32_t *fa, OffT *dfb,
+                         int32_t *dfa, bool host, OffT *X, int32_t *ba, bool atomic) {
+    cudaStream_t s = c->stream, s2 = c->stream2;
+    int pc = 0, pf = 0;  // resident CTAs per SM of each kernel: a full grid
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pc, k_rev_count<OffT>, kBlock, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pf, k_rev_fill<OffT>, kBlock, 0);
+    const int gc = std::max(1, pc) * c->nsm, gf = std::max(1, pf) * c->nsm;
+    for (int k = 0; k < kUpChunks; ++k)
+        if (!c->ev_up[k] && cudaEventCreateWithFlags(&c->ev_up[k], cudaEventDisableTiming) != cudaSuccess)
+            return ISPAN_ERR_CUDA;
+    size_t need = 0;
+    CK(cub::DeviceScan::InclusiveSum(nullptr, need, X, X, (int)V, s));
+    if (need > c->scan_tmp_bytes) {
+        if (c->scan_tmp) cudaFree(c->scan_tmp);
+        c->scan_tmp = nullptr;
+        c->scan_tmp_bytes = 0;
+        if (cudaMalloc(&c->scan_tmp, need) != cudaSuccess) return ISPAN_ERR_NOMEM;
+        c->scan_tmp_bytes = need;
+    }
+    // below 2^31 edges, the lists by a sort where its scratch fits; the
+    // counts then go one slot up (X[w + 1]), so that their inclusive scan
+    // is the start offsets
+    const bool sorted = !atomic && E > 0 && E < INT32_MAX && ensure_rev_sort(c, E);
+    OffT *cnt = sorted ? X + 1 : X;
+    CK(cudaMemsetAsync(X, 0, (size_t)(V + 1) * sizeof(OffT), s));
+    if (host) CK(cudaMemcpyAsync(dfb, fb, (size_t)(V + 1) * sizeof(OffT), cudaMemcpyHostToDevice, s));
+    // chunks of at least 2^22 ids (a small graph's copy is one chunk: the
+    // launches would cost more than the overlap gains), boundaries on
+    // multiples of four ids (the count reads int4)
+    const int nch = (int)std::max<int64_t>(1, std::min<int64_t>(kUpChunks, E >> 22));
+    const int64_t step = ((E + nch - 1) / nch + 3) / 4 * 4;
+    for (int k = 0; k < nch; ++k) {
+        const int64_t e0 = std::min<int64_t>(E, k * step), e1 = std::min<int64_t>(E, e0 + step);
+        if (host && e1 > e0)
+            CK(cudaMemcpyAsync(dfa + e0, fa + e0, (size_t)(e1 - e0) * 4, cudaMemcpyHostToDevice, s));
+        CK(cudaEventRecord(c->ev_up[k], s));
+        CK(cudaStreamWaitEvent(s2, c->ev_up[k], 0));
+        if (e1 > e0) {
+            k_rev_count<OffT><<<gc, kBlock, 0, s2>>>(dfa, e0, e1, V, cnt);
+            CK(cudaGetLastError());
+        }
+    }
+    CK(cudaEventRecord(c->ev_join, s2));
+    CK(cudaStreamWaitEvent(s, c->ev_join, 0));
+    if (V > 0) CK(cub::DeviceScan::InclusiveSum(c->scan_tmp, need, cnt, cnt, (int)V, s));
+    if (!sorted) {
+        k_rev_fill<OffT><<<gf, kBlock, 0, s>>>(dfb, dfa, V, E, X, ba);
+        CK(cudaGetLastError());
+        return ISPAN_OK;
+    }
+    int bits = 1;
+    while (bits < 31 && (1ll << bits) < V) ++bits;
+    CK(cudaMemcpyAsync(c->rv_k0, dfa, (size_t)E * 4, cudaMemcpyDeviceToDevice, s));
+    // the sources start in the output: after an even number of passes the
+    // sorted values are back there (otherwise one copy)
+    k_rev_sources<OffT><<<gf, kBlock, 0, s>>>(dfb, V, E, ba);
+    CK(cudaGetLastError());
+    cub::DoubleBuffer<int32_t> keys(c->rv_k0, c->rv_k1), vals(ba, c->rv_v);
+    size_t tb = c->rv_tmp_bytes;
+    CK(cub::DeviceRadixSort::SortPairs(c->rv_tmp, tb, keys, vals, (int)E, 0, bits, s));
+    if (vals.Current() != ba) CK(cudaMemcpyAsync(ba, vals.Current(), (size_t)E * 4, cudaMemcpyDeviceToDevice, s));
+    return ISPAN_OK;
+}
+
+// device buffers of an uploaded graph (and of a reverse CSR built here),
+// grown on demand
+static int ensure_up(ispan_ctx *c, int64_t V, int64_t E) {
+    if (c->up_V >= V && c->up_E >= E && c->up_fw_beg != nullptr) return ISPAN_OK;
+    for (void *p : c->csr_owned) cudaFree(p);
+    c->csr_owned.clear();
+    int rc = 0;
+    char *a = nullptr, *b = nullptr;
+    rc |= dalloc(&a, (size_t)(V + 1) * 8, c->csr_owned);
+    rc |= dalloc(&b, (size_t)(V + 1) * 8, c->csr_owned);
+    rc |= dalloc(&c->up_fw_adj, (size_t)E, c->csr_owned);
+    rc |= dalloc(&c->up_bw_adj, (size_t)E, c->csr_owned);
+    if (rc) {
+        c->up_V = c->up_E = -1;
+        c->up_fw_beg = nullptr;
+        return ISPAN_ERR_NOMEM;
+    }
+    c->up_fw_beg = a;
+    c->up_bw_beg = b;
+    c->up_V = V;
+    c->up_E = E;
+    return ISPAN_OK;
+}
+
+// Host input: the copies' sizes come from V and E alone; the offsets and ids
+// are checked on the device before any stage reads them.  A forward-only
+// graph is copied in one direction and its reverse built on the device.
+static int upload(ispan_ctx *c, const ispan_csr *g, bool atomic) {
+    int rc = ensure_up(c, g->V, g->E);
+    if (rc) return rc;
+    if (fw_only(g)) {
+        if (g->offset_bytes == 4)
+            return build_reverse<int32_t>(c, g->V, g->E, (const int32_t *)g->fw_beg, g->fw_adj,
+                                          (int32_t *)c->up_fw_beg, c->up_fw_adj, true, (int32_t *)c->up_bw_beg,
+                                          c->up_bw_adj, atomic);
+        return build_reverse<int64_t>(c, g->V, g->E, (const int64_t *)g->fw_beg, g->fw_adj, (int64_t *)c->up_fw_beg,
+                                      c->up_fw_adj, true, (int64_t *)c->up_bw_beg, c->up_bw_adj, atomic);
+    }
+    size_t ob = (size_t)g->offset_bytes;
     CK(cudaMemcpyAsync(c->up_fw_beg, g->fw_beg, (size_t)(g->V + 1) * ob, cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(c->up_bw_beg, g->bw_beg, (size_t)(g->V + 1) * ob, cudaMemcpyHostToDevice, c->stream));
     if (g->E) {
@@ -887,7 +1023,7 @@ static int upload(ispan_ctx *c, const ispan_csr *g) {
 // the body of a run; the caller holds c->mu and has made c->device current
 static int run_locked(ispan_ctx *c, const ispan_csr *g, int32_t nseg, const int64_t *vbase_host,
                       const ispan_params *p, int32_t *labels_out, ispan_stats *st) {
-    int rc = check_csr(g);
+    int rc = check_csr(g, true);
     if (rc) return rc;
     if (g->V > c->maxV || g->E > c->maxE) return ISPAN_ERR_CAPACITY;
     if (nseg < 1) return ISPAN_ERR_ARG;
@@ -908,16 +1044,33 @@ static int run_locked(ispan_ctx *c, const ispan_csr *g, int32_t nseg, const int6
     }
     const void *fwb = g->fw_beg, *bwb = g->bw_beg;
     const int32_t *fwa = g->fw_adj, *bwa = g->bw_adj;
+    const bool atomic = p && (p->flags & ISPAN_F_REVERSE_ATOMIC);
     if (!g->on_device) {
         // the copies' sizes come from V and E alone; the offsets (monotone,
         // from 0 to E) and the ids of host input are checked on the device,
         // before any stage reads them (a serial host scan of the offsets
         // cost more than the upload itself on large graphs)
-        if ((rc = upload(c, g))) return rc;
+        if ((rc = upload(c, g, atomic))) return rc;
         c->validate_next = true;
         fwb = c->up_fw_beg;
         bwb = c->up_bw_beg;
         fwa = c->up_fw_adj;
+        bwa = c->up_bw_adj;
+    } else if (fw_only(g)) {
+        // device input in one direction: the reverse goes to the upload
+        // buffers, and the whole graph is checked before the stages
+        if ((rc = ensure_up(c, g->V, g->E))) return rc;
+        if (g->offset_bytes == 4)
+            rc = build_reverse<int32_t>(c, g->V, g->E, (const int32_t *)fwb, fwa, (int32_t *)fwb,
+                                        const_cast<int32_t *>(fwa), false, (int32_t *)c->up_bw_beg, c->up_bw_adj,
+                                        atomic);
+        else
+            rc = build_reverse<int64_t>(c, g->V, g->E, (const int64_t *)fwb, fwa, (int64_t *)fwb,
+                                        const_cast<int32_t *>(fwa), false, (int64_t *)c->up_bw_beg, c->up_bw_adj,
+                                        atomic);
+        if (rc) return rc;
+        c->validate_next = true;
+        bwb = c->up_bw_beg;
         bwa = c->up_bw_adj;
     }
     const bool dev_labels = p && (p->flags & ISPAN_F_LABELS_ON_DEVICE);
@@ -1281,6 +1434,10 @@ int ispan_ctx_destroy(ispan_ctx *c) {
     }
     if (c->ev_fork) cudaEventDestroy(c->ev_fork);
     if (c->ev_join) cudaEventDestroy(c->ev_join);
+    for (int k = 0; k < kUpChunks; ++k)
+        if (c->ev_up[k]) cudaEventDestroy(c->ev_up[k]);
+    if (c->scan_tmp) cudaFree(c->scan_tmp);
+    for (void *p : c->rv_owned) cudaFree(p);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return ISPAN_OK;
