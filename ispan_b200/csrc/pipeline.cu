@@ -902,6 +902,13 @@ static bool ensure_rev_sort(ispan_ctx *c, int64_t E) {
     return true;
 }
 
+// the verdict of the reverse build's checks on the forward CSR
+static int rev_checked(ispan_ctx *c) {
+    CK(cudaMemcpyAsync(c->h_err + 2, c->err + 2, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return c->h_err[2] ? ISPAN_ERR_ARG : ISPAN_OK;
+}
+
 // The reverse CSR (X = reverse offsets, ba = reverse adjacency) of the
 // forward CSR (fb, fa) on the device.  With `host` set, fb and fa are host
 // arrays: the offsets and then the adjacency, in kUpChunks chunks, are
@@ -927,6 +934,8 @@ static int build_reverse(ispan_ctx *c, int64_t V, int64_t E, const OffT *fb, con
         if (cudaMalloc(&c->scan_tmp, need) != cudaSuccess) return ISPAN_ERR_NOMEM;
         c->scan_tmp_bytes = need;
     }
+    int *bad = c->err + 2;  // a malformed forward CSR, seen by the passes below
+    CK(cudaMemsetAsync(bad, 0, sizeof(int), s));
     // below 2^31 edges, the lists by a sort where its scratch fits; the
     // counts then go one slot up (X[w + 1]), so that their inclusive scan
     // is the start offsets
@@ -934,6 +943,16 @@ static int build_reverse(ispan_ctx *c, int64_t V, int64_t E, const OffT *fb, con
     OffT *cnt = sorted ? X + 1 : X;
     CK(cudaMemsetAsync(X, 0, (size_t)(V + 1) * sizeof(OffT), s));
     if (host) CK(cudaMemcpyAsync(dfb, fb, (size_t)(V + 1) * sizeof(OffT), cudaMemcpyHostToDevice, s));
+    if (sorted) {
+        // the sort's values (each edge's source) need the offsets only: they
+        // are written while the adjacency is still being copied.  The
+        // sources start in the output: after an even number of passes the
+        // sorted values are back there (otherwise one copy)
+        CK(cudaEventRecord(c->ev_fork, s));
+        CK(cudaStreamWaitEvent(s2, c->ev_fork, 0));
+        k_rev_sources<OffT><<<gf, kBlock, 0, s2>>>(dfb, V, E, ba, bad);
+        CK(cudaGetLastError());
+    }
     // chunks of at least 2^22 ids (a small graph's copy is one chunk: the
     // launches would cost more than the overlap gains), boundaries on
     // multiples of four ids (the count reads int4)
@@ -946,30 +965,28 @@ static int build_reverse(ispan_ctx *c, int64_t V, int64_t E, const OffT *fb, con
         CK(cudaEventRecord(c->ev_up[k], s));
         CK(cudaStreamWaitEvent(s2, c->ev_up[k], 0));
         if (e1 > e0) {
-            k_rev_count<OffT><<<gc, kBlock, 0, s2>>>(dfa, e0, e1, V, cnt);
+            k_rev_count<OffT><<<gc, kBlock, 0, s2>>>(dfa, e0, e1, V, cnt, bad);
             CK(cudaGetLastError());
+            // the sort's keys: a copy of the forward ids (they must survive)
+            if (sorted)
+                CK(cudaMemcpyAsync(c->rv_k0 + e0, dfa + e0, (size_t)(e1 - e0) * 4, cudaMemcpyDeviceToDevice, s2));
         }
     }
     CK(cudaEventRecord(c->ev_join, s2));
     CK(cudaStreamWaitEvent(s, c->ev_join, 0));
     if (V > 0) CK(cub::DeviceScan::InclusiveSum(c->scan_tmp, need, cnt, cnt, (int)V, s));
     if (!sorted) {
-        k_rev_fill<OffT><<<gf, kBlock, 0, s>>>(dfb, dfa, V, E, X, ba);
+        k_rev_fill<OffT><<<gf, kBlock, 0, s>>>(dfb, dfa, V, E, X, ba, bad);
         CK(cudaGetLastError());
-        return ISPAN_OK;
+        return rev_checked(c);
     }
     int bits = 1;
     while (bits < 31 && (1ll << bits) < V) ++bits;
-    CK(cudaMemcpyAsync(c->rv_k0, dfa, (size_t)E * 4, cudaMemcpyDeviceToDevice, s));
-    // the sources start in the output: after an even number of passes the
-    // sorted values are back there (otherwise one copy)
-    k_rev_sources<OffT><<<gf, kBlock, 0, s>>>(dfb, V, E, ba);
-    CK(cudaGetLastError());
     cub::DoubleBuffer<int32_t> keys(c->rv_k0, c->rv_k1), vals(ba, c->rv_v);
     size_t tb = c->rv_tmp_bytes;
     CK(cub::DeviceRadixSort::SortPairs(c->rv_tmp, tb, keys, vals, (int)E, 0, bits, s));
     if (vals.Current() != ba) CK(cudaMemcpyAsync(ba, vals.Current(), (size_t)E * 4, cudaMemcpyDeviceToDevice, s));
-    return ISPAN_OK;
+    return rev_checked(c);
 }
 
 // device buffers of an uploaded graph (and of a reverse CSR built here),
@@ -1051,14 +1068,15 @@ static int run_locked(ispan_ctx *c, const ispan_csr *g, int32_t nseg, const int6
         // before any stage reads them (a serial host scan of the offsets
         // cost more than the upload itself on large graphs)
         if ((rc = upload(c, g, atomic))) return rc;
-        c->validate_next = true;
+        // a forward-only graph was checked while its reverse was built
+        c->validate_next = !fw_only(g) || g->V == 0;
         fwb = c->up_fw_beg;
         bwb = c->up_bw_beg;
         fwa = c->up_fw_adj;
         bwa = c->up_bw_adj;
     } else if (fw_only(g)) {
         // device input in one direction: the reverse goes to the upload
-        // buffers, and the whole graph is checked before the stages
+        // buffers, and the forward CSR is checked while it is built
         if ((rc = ensure_up(c, g->V, g->E))) return rc;
         if (g->offset_bytes == 4)
             rc = build_reverse<int32_t>(c, g->V, g->E, (const int32_t *)fwb, fwa, (int32_t *)fwb,
@@ -1069,7 +1087,7 @@ static int run_locked(ispan_ctx *c, const ispan_csr *g, int32_t nseg, const int6
                                         const_cast<int32_t *>(fwa), false, (int64_t *)c->up_bw_beg, c->up_bw_adj,
                                         atomic);
         if (rc) return rc;
-        c->validate_next = true;
+        c->validate_next = g->V == 0;  // checked while the reverse was built
         bwb = c->up_bw_beg;
         bwa = c->up_bw_adj;
     }

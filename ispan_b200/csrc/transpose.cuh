@@ -14,21 +14,38 @@
 // array; lists in no particular order -- the stages never depend on
 // adjacency order).
 //
-// Malformed input must not make these kernels touch memory outside the
-// arrays: ids outside [0, V) are skipped, a vertex whose offsets are not
+// These passes read every forward offset and id, so they also check them
+// (offsets from 0 to E, never falling; ids in [0, V)) and raise *bad
+// otherwise: the reverse built from a good forward CSR is good by
+// construction, and the separate input check (k_validate) is not needed.
+// Malformed input must not make them touch memory outside the arrays: ids
+// outside [0, V) are skipped, a vertex whose offsets are not
 // 0 <= beg <= end <= E places nothing, and a placement outside [0, E) is
-// dropped.  The input check that runs before any stage (k_validate) then
-// refuses the graph.
+// dropped; the run is then refused.
 #pragma once
 #include "common.cuh"
 
 namespace ispan {
 
 template <typename OffT>
-__device__ __forceinline__ void rev_bump(OffT *X, int32_t w, int64_t V) {
-    if ((uint64_t)(int64_t)w >= (uint64_t)V) return;
+__device__ __forceinline__ void rev_bump(OffT *X, int32_t w, int64_t V, bool &bad) {
+    if ((uint64_t)(int64_t)w >= (uint64_t)V) {
+        bad = true;
+        return;
+    }
     if (sizeof(OffT) == 8) atomicAdd(reinterpret_cast<unsigned long long *>(X + w), 1ull);
     else atomicAdd(reinterpret_cast<int *>(X + w), 1);
+}
+
+// the offsets of source u, checked: [a, b) with 0 <= a <= b <= E, the first
+// offset 0 and the last E; otherwise an empty range and false
+template <typename OffT>
+__device__ __forceinline__ bool rev_range(const OffT *fb, int64_t u, int64_t V, int64_t E, int64_t &a, int64_t &b) {
+    a = (int64_t)fb[u];
+    b = (int64_t)fb[u + 1];
+    const bool ok = 0 <= a && a <= b && b <= E && (u != 0 || a == 0) && (u != V - 1 || b == E);
+    if (!ok) a = b = 0;
+    return ok;
 }
 
 // The second way to the reverse lists, used where its scratch fits: a copy
@@ -39,18 +56,16 @@ __device__ __forceinline__ void rev_bump(OffT *X, int32_t w, int64_t V) {
 // less once the offsets exceed L2).  This fills the values: vals[e] = u for
 // the edges e of every source u.
 template <typename OffT>
-__global__ void __launch_bounds__(kBlock) k_rev_sources(const OffT *fb, int64_t V, int64_t E, int32_t *vals) {
+__global__ void __launch_bounds__(kBlock) k_rev_sources(const OffT *fb, int64_t V, int64_t E, int32_t *vals,
+                                                        int *bad) {
     const int lane = lane_id();
     const int64_t gw = ((int64_t)blockIdx.x * kBlock + threadIdx.x) >> 5;
     const int64_t nw = ((int64_t)gridDim.x * kBlock) >> 5;
+    bool bd = false;
     for (int64_t base = gw * 32; base < V; base += nw * 32) {
         const int64_t u = base + lane;
         int64_t a = 0, b = 0;
-        if (u < V) {
-            a = (int64_t)fb[u];
-            b = (int64_t)fb[u + 1];
-            if (!(0 <= a && a <= b && b <= E)) a = b = 0;
-        }
+        if (u < V) bd |= !rev_range(fb, u, V, E, a, b);
         const bool big = b - a >= 32;
         if (!big)
             for (int64_t e = a; e < b; ++e) vals[e] = (int32_t)u;
@@ -60,24 +75,27 @@ __global__ void __launch_bounds__(kBlock) k_rev_sources(const OffT *fb, int64_t 
             for (int64_t e = s0 + lane; e < s1; e += 32) vals[e] = (int32_t)(base + src);
         }
     }
+    if (__syncthreads_or(bd) && threadIdx.x == 0) atomicExch(bad, 1);
 }
 
 // in-degree counts X[w] += 1 for the edges adj[e0, e1); where adj + e0 is
 // 16-byte aligned the body is read as int4 (each id read once, streamed)
 template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_rev_count(const int32_t *adj, int64_t e0, int64_t e1, int64_t V,
-                                                      OffT *X) {
+                                                      OffT *X, int *bad) {
     const int64_t gt = (int64_t)blockIdx.x * kBlock + threadIdx.x, nt = (int64_t)gridDim.x * kBlock;
     const int64_t nq = ((uintptr_t)(adj + e0) & 15) ? 0 : (e1 - e0) >> 2;
     const int4 *q = reinterpret_cast<const int4 *>(adj + e0);
+    bool b = false;
     for (int64_t i = gt; i < nq; i += nt) {
         const int4 w = __ldcs(q + i);
-        rev_bump(X, w.x, V);
-        rev_bump(X, w.y, V);
-        rev_bump(X, w.z, V);
-        rev_bump(X, w.w, V);
+        rev_bump(X, w.x, V, b);
+        rev_bump(X, w.y, V, b);
+        rev_bump(X, w.z, V, b);
+        rev_bump(X, w.w, V, b);
     }
-    for (int64_t e = e0 + (nq << 2) + gt; e < e1; e += nt) rev_bump(X, __ldcs(adj + e), V);
+    for (int64_t e = e0 + (nq << 2) + gt; e < e1; e += nt) rev_bump(X, __ldcs(adj + e), V, b);
+    if (__syncthreads_or(b) && threadIdx.x == 0) atomicExch(bad, 1);
 }
 
 template <typename OffT>
@@ -111,19 +129,16 @@ __device__ __forceinline__ void rev_place(OffT *X, int32_t *ba, const int32_t *f
 // by their own lane, longer ones by the whole warp in turn (coalesced reads).
 template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_rev_fill(const OffT *fb, const int32_t *fa, int64_t V, int64_t E, OffT *X,
-                                                     int32_t *ba) {
+                                                     int32_t *ba, int *bad) {
     if (blockIdx.x == 0 && threadIdx.x == 0) X[V] = (OffT)E;
     const int lane = lane_id();
     const int64_t gw = ((int64_t)blockIdx.x * kBlock + threadIdx.x) >> 5;
     const int64_t nw = ((int64_t)gridDim.x * kBlock) >> 5;
+    bool bd = false;
     for (int64_t base = gw * 32; base < V; base += nw * 32) {
         const int64_t u = base + lane;
         int64_t a = 0, b = 0;
-        if (u < V) {
-            a = (int64_t)fb[u];
-            b = (int64_t)fb[u + 1];
-            if (!(0 <= a && a <= b && b <= E)) a = b = 0;
-        }
+        if (u < V) bd |= !rev_range(fb, u, V, E, a, b);
         const bool big = b - a >= 32;
         if (!big) rev_place(X, ba, fa, a, b, 1, (int32_t)u, V, E);
         for (unsigned m = __ballot_sync(kFull, big); m; m &= m - 1) {
@@ -132,6 +147,7 @@ __global__ void __launch_bounds__(kBlock) k_rev_fill(const OffT *fb, const int32
             rev_place(X, ba, fa, s0 + lane, s1, 32, (int32_t)(base + src), V, E);
         }
     }
+    if (__syncthreads_or(bd) && threadIdx.x == 0) atomicExch(bad, 1);
 }
 
 }  // namespace ispan
