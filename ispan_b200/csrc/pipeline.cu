@@ -153,12 +153,15 @@ struct ispan_ctx {
     cudaEvent_t ev_up[kUpChunks] = {};  // forward adjacency chunk k copied
     void *scan_tmp = nullptr;           // the reverse offsets' scan
     size_t scan_tmp_bytes = 0;
-    // the reverse lists by a radix sort of (id, source) pairs: keys, their
-    // alternate, the sources' alternate, and the sort's temporary storage
-    int32_t *rv_k0 = nullptr, *rv_k1 = nullptr, *rv_v = nullptr;
+    // the reverse lists by a radix sort of (id, source) pairs, chunk by
+    // chunk: keys and sources of all edges, a chunk's alternates, the
+    // running in-degree counts after each chunk, a chunk's run starts, and
+    // the sort's and scan's temporary storage
+    int32_t *rv_k0 = nullptr, *rv_v = nullptr, *rv_k1 = nullptr, *rv_v1 = nullptr;
+    int32_t *rv_snap = nullptr, *rv_run = nullptr;
     void *rv_tmp = nullptr;
     size_t rv_tmp_bytes = 0;
-    int64_t rv_E = -1;
+    int64_t rv_E = -1, rv_V = -1;
     bool rv_failed = false;  // the scratch did not fit: placement by atomics
     std::vector<void *> rv_owned;
 
@@ -875,29 +878,49 @@ static int check_csr(const ispan_csr *g, bool allow_fw_only = false) {
     return ISPAN_OK;
 }
 
-// scratch of the sorted reverse lists for E edges (3 E ids and the sort's
-// storage, kept for later runs); false if it does not fit
-static bool ensure_rev_sort(ispan_ctx *c, int64_t E) {
-    if (!c->rv_failed && c->rv_E >= E) return true;
-    if (c->rv_failed && E >= c->rv_E) return false;
+// chunks of the forward adjacency's copy: at least 2^22 ids each (a small
+// graph's copy is one chunk: the launches would cost more than the overlap
+// gains), at most kUpChunks, boundaries on multiples of four ids (the count
+// reads int4)
+static int up_chunks(int64_t E, int64_t *step) {
+    const int nch = (int)std::max<int64_t>(1, std::min<int64_t>(kUpChunks, E >> 22));
+    *step = ((E + nch - 1) / nch + 3) / 4 * 4;
+    return nch;
+}
+
+// scratch of the sorted reverse lists for V vertices and E edges (2 E ids,
+// two chunks' alternates, kUpChunks + 1 arrays of V counts, the sort's and
+// the scan's storage; kept for later runs); false if it does not fit
+static bool ensure_rev_sort(ispan_ctx *c, int64_t V, int64_t E) {
+    if (!c->rv_failed && c->rv_E >= E && c->rv_V >= V) return true;
+    if (c->rv_failed && E >= c->rv_E && V >= c->rv_V) return false;
     for (void *p : c->rv_owned) cudaFree(p);
     c->rv_owned.clear();
-    c->rv_E = -1;
-    size_t tb = 0;
+    c->rv_E = c->rv_V = -1;
+    int64_t step = 0;
+    up_chunks(E, &step);
+    size_t tb = 0, ts = 0;
     cub::DoubleBuffer<int32_t> k(nullptr, nullptr), v(nullptr, nullptr);
-    bool ok = cub::DeviceRadixSort::SortPairs(nullptr, tb, k, v, (int)E, 0, 32, c->stream) == cudaSuccess;
-    ok = ok && dalloc(&c->rv_k0, (size_t)E, c->rv_owned) == 0 && dalloc(&c->rv_k1, (size_t)E, c->rv_owned) == 0 &&
-         dalloc(&c->rv_v, (size_t)E, c->rv_owned) == 0 && dalloc((char **)&c->rv_tmp, tb, c->rv_owned) == 0;
+    bool ok = cub::DeviceRadixSort::SortPairs(nullptr, tb, k, v, (int)step, 0, 32, c->stream) == cudaSuccess &&
+              cub::DeviceScan::ExclusiveSum(nullptr, ts, (int32_t *)nullptr, (int32_t *)nullptr, (int)V,
+                                            c->stream) == cudaSuccess;
+    tb = std::max(tb, ts);
+    ok = ok && dalloc(&c->rv_k0, (size_t)E, c->rv_owned) == 0 && dalloc(&c->rv_v, (size_t)E, c->rv_owned) == 0 &&
+         dalloc(&c->rv_k1, (size_t)step, c->rv_owned) == 0 && dalloc(&c->rv_v1, (size_t)step, c->rv_owned) == 0 &&
+         dalloc(&c->rv_snap, (size_t)kUpChunks * V, c->rv_owned) == 0 &&
+         dalloc(&c->rv_run, (size_t)V, c->rv_owned) == 0 && dalloc((char **)&c->rv_tmp, tb, c->rv_owned) == 0;
     if (!ok) {
         for (void *p : c->rv_owned) cudaFree(p);
         c->rv_owned.clear();
         cudaGetLastError();  // a failed allocation is not an error of the run
         c->rv_failed = true;
         c->rv_E = E;  // this size (and larger) takes the atomic placement
+        c->rv_V = V;
         return false;
     }
     c->rv_tmp_bytes = tb;
     c->rv_E = E;
+    c->rv_V = V;
     c->rv_failed = false;
     return true;
 }
@@ -939,25 +962,25 @@ static int build_reverse(ispan_ctx *c, int64_t V, int64_t E, const OffT *fb, con
     // below 2^31 edges, the lists by a sort where its scratch fits; the
     // counts then go one slot up (X[w + 1]), so that their inclusive scan
     // is the start offsets
-    const bool sorted = !atomic && E > 0 && E < INT32_MAX && ensure_rev_sort(c, E);
+    const bool sorted = !atomic && E > 0 && E < INT32_MAX && ensure_rev_sort(c, V, E);
     OffT *cnt = sorted ? X + 1 : X;
+    int bits = 1;  // key bits of the sort: ids below V
+    while (bits < 31 && (1ll << bits) < V) ++bits;
+    int64_t step = 0;
+    const int nch = up_chunks(E, &step);
     CK(cudaMemsetAsync(X, 0, (size_t)(V + 1) * sizeof(OffT), s));
     if (host) CK(cudaMemcpyAsync(dfb, fb, (size_t)(V + 1) * sizeof(OffT), cudaMemcpyHostToDevice, s));
     if (sorted) {
         // the sort's values (each edge's source) need the offsets only: they
-        // are written while the adjacency is still being copied.  The
-        // sources start in the output: after an even number of passes the
-        // sorted values are back there (otherwise one copy)
+        // are written while the adjacency is still being copied
         CK(cudaEventRecord(c->ev_fork, s));
         CK(cudaStreamWaitEvent(s2, c->ev_fork, 0));
-        k_rev_sources<OffT><<<gf, kBlock, 0, s2>>>(dfb, V, E, ba, bad);
+        k_rev_sources<OffT><<<gf, kBlock, 0, s2>>>(dfb, V, E, c->rv_v, bad);
         CK(cudaGetLastError());
     }
-    // chunks of at least 2^22 ids (a small graph's copy is one chunk: the
-    // launches would cost more than the overlap gains), boundaries on
-    // multiples of four ids (the count reads int4)
-    const int nch = (int)std::max<int64_t>(1, std::min<int64_t>(kUpChunks, E >> 22));
-    const int64_t step = ((E + nch - 1) / nch + 3) / 4 * 4;
+    // each chunk, as soon as it has landed: its in-degree counts and, for the
+    // sort, a snapshot of the running counts, its keys (a copy of the ids:
+    // the forward lists must survive) and its own stable sort
     for (int k = 0; k < nch; ++k) {
         const int64_t e0 = std::min<int64_t>(E, k * step), e1 = std::min<int64_t>(E, e0 + step);
         if (host && e1 > e0)
@@ -967,9 +990,20 @@ static int build_reverse(ispan_ctx *c, int64_t V, int64_t E, const OffT *fb, con
         if (e1 > e0) {
             k_rev_count<OffT><<<gc, kBlock, 0, s2>>>(dfa, e0, e1, V, cnt, bad);
             CK(cudaGetLastError());
-            // the sort's keys: a copy of the forward ids (they must survive)
-            if (sorted)
-                CK(cudaMemcpyAsync(c->rv_k0 + e0, dfa + e0, (size_t)(e1 - e0) * 4, cudaMemcpyDeviceToDevice, s2));
+        }
+        if (!sorted) continue;
+        k_rev_snap<OffT><<<gf, kBlock, 0, s2>>>(cnt, V, c->rv_snap + (size_t)k * V);
+        CK(cudaGetLastError());
+        if (e1 > e0) {
+            const int n = (int)(e1 - e0);
+            CK(cudaMemcpyAsync(c->rv_k0 + e0, dfa + e0, (size_t)n * 4, cudaMemcpyDeviceToDevice, s2));
+            cub::DoubleBuffer<int32_t> keys(c->rv_k0 + e0, c->rv_k1), vals(c->rv_v + e0, c->rv_v1);
+            size_t tb = c->rv_tmp_bytes;
+            CK(cub::DeviceRadixSort::SortPairs(c->rv_tmp, tb, keys, vals, n, 0, bits, s2));
+            if (keys.Current() != c->rv_k0 + e0)
+                CK(cudaMemcpyAsync(c->rv_k0 + e0, keys.Current(), (size_t)n * 4, cudaMemcpyDeviceToDevice, s2));
+            if (vals.Current() != c->rv_v + e0)
+                CK(cudaMemcpyAsync(c->rv_v + e0, vals.Current(), (size_t)n * 4, cudaMemcpyDeviceToDevice, s2));
         }
     }
     CK(cudaEventRecord(c->ev_join, s2));
@@ -980,12 +1014,19 @@ static int build_reverse(ispan_ctx *c, int64_t V, int64_t E, const OffT *fb, con
         CK(cudaGetLastError());
         return rev_checked(c);
     }
-    int bits = 1;
-    while (bits < 31 && (1ll << bits) < V) ++bits;
-    cub::DoubleBuffer<int32_t> keys(c->rv_k0, c->rv_k1), vals(ba, c->rv_v);
-    size_t tb = c->rv_tmp_bytes;
-    CK(cub::DeviceRadixSort::SortPairs(c->rv_tmp, tb, keys, vals, (int)E, 0, bits, s));
-    if (vals.Current() != ba) CK(cudaMemcpyAsync(ba, vals.Current(), (size_t)E * 4, cudaMemcpyDeviceToDevice, s));
+    // each chunk's sorted runs into place: run starts inside the chunk (the
+    // exclusive scan of its own counts), then the pairs
+    for (int k = 0; k < nch; ++k) {
+        const int64_t e0 = std::min<int64_t>(E, k * step), e1 = std::min<int64_t>(E, e0 + step);
+        if (e1 <= e0) continue;
+        const int32_t *before = k ? c->rv_snap + (size_t)(k - 1) * V : nullptr;
+        k_rev_diff<<<gf, kBlock, 0, s>>>(c->rv_snap + (size_t)k * V, before, V, c->rv_run);
+        CK(cudaGetLastError());
+        size_t tb = c->rv_tmp_bytes;
+        CK(cub::DeviceScan::ExclusiveSum(c->rv_tmp, tb, c->rv_run, c->rv_run, (int)V, s));
+        k_rev_runs<OffT><<<gf, kBlock, 0, s>>>(c->rv_k0 + e0, c->rv_v + e0, e1 - e0, X, before, c->rv_run, V, ba);
+        CK(cudaGetLastError());
+    }
     return rev_checked(c);
 }
 

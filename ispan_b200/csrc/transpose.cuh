@@ -78,6 +78,45 @@ __global__ void __launch_bounds__(kBlock) k_rev_sources(const OffT *fb, int64_t 
     if (__syncthreads_or(bd) && threadIdx.x == 0) atomicExch(bad, 1);
 }
 
+// The sort runs chunk by chunk while the next chunk is still being copied:
+// chunk k's (id, source) pairs are sorted on their own (stable), and after
+// the last chunk each chunk's runs are placed.  Edges to w from chunk k go
+// after those from chunks 0..k-1 (lists stay in increasing source order:
+// chunks are in edge order, edges in source order); their offset inside w's
+// list is the running in-degree count before chunk k, snapshotted after each
+// chunk's count (k_rev_snap), and their offset inside chunk k's sorted run is
+// the exclusive scan of chunk k's own counts (k_rev_diff, then a scan).
+
+// snap[w] = the running in-degree count of w (cnt[w] as int32)
+template <typename OffT>
+__global__ void __launch_bounds__(kBlock) k_rev_snap(const OffT *cnt, int64_t V, int32_t *snap) {
+    for (int64_t w = (int64_t)blockIdx.x * kBlock + threadIdx.x; w < V; w += (int64_t)gridDim.x * kBlock)
+        snap[w] = (int32_t)cnt[w];
+}
+
+// d[w] = chunk k's own count of w: snapshot after it minus snapshot before it
+__global__ void __launch_bounds__(kBlock) k_rev_diff(const int32_t *after, const int32_t *before, int64_t V,
+                                                     int32_t *d) {
+    for (int64_t w = (int64_t)blockIdx.x * kBlock + threadIdx.x; w < V; w += (int64_t)gridDim.x * kBlock)
+        d[w] = after[w] - (before ? before[w] : 0);
+}
+
+// place chunk k's sorted pairs (keys[i], vals[i]), i < n: the pair is the
+// (i - run[w])-th of the chunk's edges to w, which follow the before[w]
+// edges to w of the earlier chunks in w's list starting at X[w].  A slot
+// outside w's list (only on malformed input) is dropped.
+template <typename OffT>
+__global__ void __launch_bounds__(kBlock) k_rev_runs(const int32_t *keys, const int32_t *vals, int64_t n,
+                                                     const OffT *X, const int32_t *before, const int32_t *run,
+                                                     int64_t V, int32_t *ba) {
+    for (int64_t i = (int64_t)blockIdx.x * kBlock + threadIdx.x; i < n; i += (int64_t)gridDim.x * kBlock) {
+        const int32_t w = keys[i];
+        if ((uint64_t)(int64_t)w >= (uint64_t)V) continue;
+        const int64_t pos = (int64_t)X[w] + (before ? before[w] : 0) + (i - run[w]);
+        if (pos >= (int64_t)X[w] && pos < (int64_t)X[w + 1]) ba[pos] = vals[i];
+    }
+}
+
 // in-degree counts X[w] += 1 for the edges adj[e0, e1); where adj + e0 is
 // 16-byte aligned the body is read as int4 (each id read once, streamed)
 template <typename OffT>
