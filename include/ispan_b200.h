@@ -40,9 +40,9 @@ extern "C" {
  * fastest).  bw_beg and bw_adj both NULL: the forward CSR alone is given (and,
  * for host memory, copied); the scc runs build the reverse on the device,
  * which halves the bytes a host graph sends over PCIe.  Below 2^31 edges, and
- * where 12 bytes an edge of scratch fit (kept by the context), its lists are
- * sorted by a radix sort (increasing source order); otherwise they are placed
- * by atomics, in no particular order.  ispan_scc_run_graphs needs both
+ * where about 9 bytes an edge of scratch fit (kept by the context), its lists
+ * are sorted by a radix sort (increasing source order); otherwise they are
+ * placed by atomics, in no particular order.  ispan_scc_run_graphs needs both
  * directions. */
 typedef struct {
     int64_t V, E;
@@ -75,7 +75,7 @@ typedef struct {
 #define ISPAN_F_EXACT_STATS 32u     /* also fill fw_edges / bw_edges and the trims' worklist
                                        sizes (extra passes) */
 #define ISPAN_F_REVERSE_ATOMIC 64u  /* forward-only input: place the reverse lists by atomics
-                                       (no sort scratch of 12 bytes an edge; slower) */
+                                       (no sort scratch; slower) */
 
 /* Stage-time slots follow the reference's avg_time[15] meanings
  * (src/scc_core.cpp:24-25, :1037-1053): 0 trim, 1 elephant SCC, 2 mice SCC,
