@@ -372,11 +372,12 @@ def e2e_plain(ctx, g, stream, steps, tun, ws):
 
 
 def e2e_pick(E, fw, both):
-    """The end-to-end record: below 2^31 edges the forward CSR alone is sent
-    (its reverse is sorted on the device, faster than copying it); larger
-    graphs send both directions (their reverse would be placed by atomics,
-    slower than the copy).  The other form is kept as a sub-record."""
-    if E < 2**31 - 1:
+    """The end-to-end record: the forward CSR alone is sent where the library
+    sorts the reverse chunk by chunk (each of its eight copy chunks below
+    2^31 edges), faster than copying the reverse; beyond that the reverse
+    would be placed by atomics, slower than the copy, and both directions
+    are sent.  The other form is kept as a sub-record."""
+    if (E + 7) // 8 < 2**31 - 1:
         return dict(fw, input="the forward CSR from pinned host memory; the reverse CSR is built on the device "
                               "inside the step", both_directions=both)
     return dict(both, input="both CSRs from pinned host memory", forward_only=fw)

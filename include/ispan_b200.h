@@ -39,10 +39,11 @@ extern "C" {
  * of the context's GPU; 0 when they are host memory (pinned memory uploads
  * fastest).  bw_beg and bw_adj both NULL: the forward CSR alone is given (and,
  * for host memory, copied); the scc runs build the reverse on the device,
- * which halves the bytes a host graph sends over PCIe.  Below 2^31 edges, and
- * where about 9 bytes an edge of scratch fit (kept by the context), its lists
- * are sorted by a radix sort (increasing source order); otherwise they are
- * placed by atomics, in no particular order.  ispan_scc_run_graphs needs both
+ * which halves the bytes a host graph sends over PCIe.  Where about 9 bytes
+ * an edge and 36 a vertex of scratch fit (kept by the context; copy chunks
+ * below 2^31 edges), its lists are sorted chunk by chunk by a radix sort
+ * (increasing source order); otherwise they are placed by atomics, in no
+ * particular order.  ispan_scc_run_graphs needs both
  * directions. */
 typedef struct {
     int64_t V, E;

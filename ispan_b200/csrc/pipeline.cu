@@ -959,15 +959,15 @@ static int build_reverse(ispan_ctx *c, int64_t V, int64_t E, const OffT *fb, con
     }
     int *bad = c->err + 2;  // a malformed forward CSR, seen by the passes below
     CK(cudaMemsetAsync(bad, 0, sizeof(int), s));
-    // below 2^31 edges, the lists by a sort where its scratch fits; the
-    // counts then go one slot up (X[w + 1]), so that their inclusive scan
-    // is the start offsets
-    const bool sorted = !atomic && E > 0 && E < INT32_MAX && ensure_rev_sort(c, V, E);
+    int64_t step = 0;
+    const int nch = up_chunks(E, &step);
+    // the lists by a sort of each chunk where the scratch fits (chunks below
+    // 2^31 edges); the counts then go one slot up (X[w + 1]), so that their
+    // inclusive scan is the start offsets
+    const bool sorted = !atomic && E > 0 && step < INT32_MAX && ensure_rev_sort(c, V, E);
     OffT *cnt = sorted ? X + 1 : X;
     int bits = 1;  // key bits of the sort: ids below V
     while (bits < 31 && (1ll << bits) < V) ++bits;
-    int64_t step = 0;
-    const int nch = up_chunks(E, &step);
     CK(cudaMemsetAsync(X, 0, (size_t)(V + 1) * sizeof(OffT), s));
     if (host) CK(cudaMemcpyAsync(dfb, fb, (size_t)(V + 1) * sizeof(OffT), cudaMemcpyHostToDevice, s));
     if (sorted) {
