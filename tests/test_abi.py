@@ -43,3 +43,15 @@ def test_version_and_errors_without_gpu():
     import torch
     if not torch.cuda.is_available():
         assert L.ispan_ctx_create(0, 10, 10, ctypes.byref(h)) == -6  # ISPAN_ERR_NODEV, no crash
+
+
+def test_flag_values_match_the_header():
+    """The Python binding's run flags carry the header's values."""
+    from ispan_b200 import _lib
+    src = open(os.path.join(ROOT, "include", "ispan_b200.h")).read()
+    flags = {m.group(1): int(m.group(2)) for m in re.finditer(r"#define ISPAN_F_(\w+)\s+(\d+)u", src)}
+    assert {"LABELS_ON_DEVICE", "VALIDATE", "EXACT_STATS", "REVERSE_ATOMIC"} <= set(flags)
+    for name, value in flags.items():
+        if hasattr(_lib, "F_" + name):
+            assert getattr(_lib, "F_" + name) == value, name
+    assert _lib.F_REVERSE_ATOMIC == flags["REVERSE_ATOMIC"]
