@@ -174,6 +174,7 @@ __device__ __forceinline__ void td_chunk(const Run<OffT> &r, const BfsDir<OffT, 
         const bool one_list = my0 + kPer <= e1 && (i + 1 >= ns || sm.qe[i + 1] >= my0 + kPer);
 #ifdef ISPAN_CHECKED
         const bool vec = false;  // the checked build range-checks every id
+        (void)one_list;
 #else
         const bool vec = kPer == 4 && one_list && ((uintptr_t)(d.xadj + p0) & 15) == 0;
 #endif
