@@ -22,7 +22,8 @@ The frontier count is summed on the device and read by the host only every
 do nothing), so the host does not wait on the GPU once per level.  Work per
 level is proportional to the frontier's edges; per level and rank the
 collectives move V bytes into the reduce-scatter and V/8 bytes out of the
-all-gather.  Only the search is sharded (the elephant stage).
+all-gather.  ``scc`` runs the whole detection on such rows: trim-1 and the
+pivot's SCC sharded, the residual gathered and solved on one GPU per rank.
 """
 from __future__ import annotations
 
@@ -164,3 +165,181 @@ def giant_scc(fw: Rows, bw: Rows, V: int, pivot: int, ops=GpuOps, device=None):
     f = reach(fw, V, [pivot], None, ops, device)
     b = reach(bw, V, [pivot], f, ops, device)
     return bits_to_map(b, V)
+
+
+# ---------------------------------------------------------------------------
+# The whole detection over sharded rows: trim-1, the pivot's SCC by the
+# sharded searches above, and the residual solved where it fits.
+#
+# The reference's MPI variant exchanges state at three points: the trim-1
+# statuses after the first trim (an all-gather of each rank's range,
+# src_mpi/scc_core.cpp:280-287), the labels after the giant's searches (a MAX
+# all-reduce of the label array, :529-535) and the labels of the small
+# components (a MAX all-reduce, :704-711).  Here the status is a packed
+# bitmap of active vertices, replicated by an all-gather of each rank's owned
+# words; the giant's label is a MIN all-reduce of its owned members' ids; and
+# the residual -- on the graphs this form is for, a small fraction next to the
+# giant -- is gathered whole to every rank and solved there by the
+# single-GPU engine (every rank gets the same labels, so no label exchange
+# is needed).  The per-round degree counts are tensor operations on the
+# rank's own rows (any device), not a kernel of this library.
+
+def _own_edges(rows: Rows, dev):
+    """Per edge of the rank's rows: its source row (local) and target (global)."""
+    import torch
+    beg = torch.as_tensor(rows.beg, device=dev).to(torch.int64)  # host arrays or device tensors
+    adj = torch.as_tensor(rows.adj, device=dev).to(torch.int64)
+    row = torch.repeat_interleave(torch.arange(rows.n, device=dev), beg[1:] - beg[:-1])
+    return row, adj
+
+
+def _bit(words, ids):
+    """Bits of the packed int32 words at vertex ids (int64 tensor) as bool."""
+    return ((words[ids >> 5] >> (ids & 31)) & 1) != 0
+
+
+def _pack(own, S: int):
+    """A bool tensor of at most S * 32 owned vertices as S int32 words."""
+    import torch
+    b = torch.zeros(S * 32, dtype=torch.int64, device=own.device)
+    b[:own.numel()] = own.to(torch.int64)
+    w = (b.view(S, 32) << torch.arange(32, device=own.device)).sum(1)
+    return (w - (w >= 1 << 31).to(torch.int64) * (1 << 32)).to(torch.int32)
+
+
+def _allgather_words(mine, out):
+    import torch.distributed as dist
+    if dist.is_available() and dist.is_initialized():
+        dist.all_gather_into_tensor(out, mine.contiguous())
+    else:
+        out[:mine.numel()] = mine
+
+
+def _allreduce(t, op):
+    import torch.distributed as dist
+    if dist.is_available() and dist.is_initialized():
+        dist.all_reduce(t, op=op)
+    return t
+
+
+def trim1(fw: Rows, bw: Rows, V: int, rounds: int = 3, device=None):
+    """Trim-1 over sharded rows (trim_1_first, src/trim_1_gfq.h:9-33, and the
+    peel rounds after it): a vertex with no active out-neighbour or no active
+    in-neighbour other than itself is its own SCC.  Returns (active bits,
+    trimmed bits), packed int32 words over V, identical on every rank.
+    `rounds` peel rounds at most: trim-1 only takes work off the later
+    stages, which find the same SCCs in what it leaves."""
+    import torch
+    import torch.distributed as dist
+    dev = device if device is not None else ("cuda" if torch.cuda.is_available() else "cpu")
+    distributed = dist.is_available() and dist.is_initialized()
+    world = dist.get_world_size() if distributed else 1
+    rank = dist.get_rank() if distributed else 0
+    S = words_per_rank(V, world)
+    v0, v1 = owned_range(V, rank, world)
+    own = torch.ones(v1 - v0, dtype=torch.bool, device=dev)
+    trimmed_own = torch.zeros(v1 - v0, dtype=torch.bool, device=dev)
+    active = torch.zeros(S * world, dtype=torch.int32, device=dev)
+    _allgather_words(_pack(own, S), active)
+    ids = torch.arange(v0, v1, device=dev)
+    ef, eb = _own_edges(fw, dev), _own_edges(bw, dev)
+    for _ in range(max(0, rounds)):
+        deg = []
+        for row, adj in (ef, eb):
+            live = _bit(active, adj) & (adj != ids[row])
+            deg.append(torch.zeros(v1 - v0, dtype=torch.int64, device=dev).index_add_(0, row, live.to(torch.int64)))
+        rem = own & ((deg[0] == 0) | (deg[1] == 0))
+        n = _allreduce(rem.sum().reshape(1).to(torch.int64), dist.ReduceOp.SUM if distributed else None)
+        if int(n.item()) == 0:
+            break
+        own &= ~rem
+        trimmed_own |= rem
+        _allgather_words(_pack(own, S), active)
+    trimmed = torch.zeros(S * world, dtype=torch.int32, device=dev)
+    _allgather_words(_pack(trimmed_own, S), trimmed)
+    return active, trimmed
+
+
+def pivot(fw: Rows, bw: Rows, V: int, active, device=None) -> int:
+    """The pivot (pivot_selection_from_fq, src/scc_common.h:92-150): the active
+    vertex of largest out-degree x in-degree, ties to the lowest id, as a MAX
+    all-reduce of a 64-bit key; -1 when no vertex is active."""
+    import torch
+    import torch.distributed as dist
+    dev = active.device
+    v0, n = fw.v0, fw.n
+    if n:
+        fb = torch.as_tensor(fw.beg, device=dev).to(torch.int64)
+        bb = torch.as_tensor(bw.beg, device=dev).to(torch.int64)
+        od, idg = fb[1:] - fb[:-1], bb[1:] - bb[:-1]
+        ids = torch.arange(v0, v0 + n, device=dev)
+        key = (torch.clamp(od * idg, max=(1 << 31) - 1) << 32) | (0xFFFFFFFF - ids)
+        key = torch.where(_bit(active, ids), key, torch.full_like(key, -1))
+        best = key.max().reshape(1)
+    else:
+        best = torch.full((1,), -1, dtype=torch.int64, device=dev)
+    distributed = dist.is_available() and dist.is_initialized()
+    best = int(_allreduce(best, dist.ReduceOp.MAX if distributed else None).item())
+    return -1 if best < 0 else 0xFFFFFFFF - (best & 0xFFFFFFFF)
+
+
+def _gpu_solve(csr):
+    from . import Context
+    with Context(max(csr.V, 1), max(csr.E, 1)) as ctx:
+        labels, _ = ctx.run_csr(csr)
+    return np.asarray(labels)
+
+
+def scc(fw: Rows, bw: Rows, V: int, solve=None, ops=GpuOps, device=None, trim_rounds: int = 3):
+    """SCC labels (minimum member id, int64 numpy array of V) of a graph whose
+    rows are sharded across the ranks, identical on every rank: sharded
+    trim-1, the pivot's SCC by the sharded searches, and the residual's
+    subgraph gathered to every rank and solved by `solve(csr) -> labels`
+    (default: the single-GPU engine)."""
+    import torch
+    import torch.distributed as dist
+    from . import graphs as G
+    dev = device if device is not None else ("cuda" if torch.cuda.is_available() else "cpu")
+    distributed = dist.is_available() and dist.is_initialized()
+    world = dist.get_world_size() if distributed else 1
+    solve = solve or _gpu_solve
+    labels = np.arange(V, dtype=np.int64)  # trimmed vertices are their own SCC
+    active, _ = trim1(fw, bw, V, trim_rounds, dev)
+    p = pivot(fw, bw, V, active, dev)
+    giant = torch.zeros_like(active)
+    if p >= 0:
+        f = reach(fw, V, [p], active, ops, dev)
+        giant = reach(bw, V, [p], f, ops, dev)
+        gm = bits_to_map(giant, V).to(torch.bool)
+        own = gm[fw.v0:fw.v0 + fw.n]
+        lo = torch.full((1,), V, dtype=torch.int64, device=dev)
+        if bool(own.any()):
+            lo[0] = int(torch.nonzero(own)[0, 0]) + fw.v0
+        gmin = int(_allreduce(lo, dist.ReduceOp.MIN if distributed else None).item())
+        labels[gm.cpu().numpy()] = gmin
+    # the residual: active, outside the giant; each rank sends its rows' edges
+    # between residual vertices, every rank builds and solves the subgraph
+    resid = bits_to_map(active & ~giant, V).to(torch.bool)
+    row, adj = _own_edges(fw, dev)
+    src = row + fw.v0
+    keep = resid[src] & resid[adj]
+    mine = torch.stack([src[keep], adj[keep]], 1).to(torch.int64)
+    if distributed:
+        cnt = torch.tensor([mine.shape[0]], dtype=torch.int64, device=dev)
+        cnts = [torch.zeros_like(cnt) for _ in range(world)]
+        dist.all_gather(cnts, cnt)
+        m = max(int(c.item()) for c in cnts)
+        pad = torch.full((m, 2), -1, dtype=torch.int64, device=dev)
+        pad[:mine.shape[0]] = mine
+        parts = [torch.empty_like(pad) for _ in range(world)]
+        dist.all_gather(parts, pad)
+        edges = torch.cat([q[:int(c.item())] for q, c in zip(parts, cnts)])
+    else:
+        edges = mine
+    ids = torch.nonzero(resid).flatten()
+    if ids.numel():
+        local = torch.searchsorted(ids, edges.reshape(-1)).reshape(-1, 2)
+        sub = G.from_edges(int(ids.numel()), local.cpu().numpy())
+        lab = np.asarray(solve(sub), np.int64)
+        labels[ids.cpu().numpy()] = ids.cpu().numpy()[lab]  # order-preserving ids: minima map to minima
+    return labels

@@ -1,7 +1,10 @@
-"""Sharded search (rows of one graph split across ranks), world size 2 over
-gloo on CPU: the per-level merge by MAX all-reduce gives every rank the
-pivot's exact SCC.  The oracle's CPU expansion stands in for the per-rank
-GPU kernel (tested on the GPU in test_gpu_sharded.py)."""
+"""Sharded search and detection (rows of one graph split across ranks), world
+sizes 2 and 3 over gloo on CPU: the per-level merge gives every rank the
+pivot's exact SCC, and the whole detection (sharded trim-1 and pivot, the
+giant, the residual gathered and solved) gives every rank the exact labels.
+The oracle's CPU expansion stands in for the per-rank GPU kernels (tested on
+the GPU in test_gpu_sharded.py) and the oracle's Tarjan for the single-GPU
+solve of the residual."""
 import datetime
 import os
 import socket
@@ -13,7 +16,7 @@ import torch.multiprocessing as mp
 
 import oracle
 from ispan_b200 import graphs as G
-from ispan_b200.sharded import bits_to_map, giant_scc, owned_range, reach, split_rows
+from ispan_b200.sharded import bits_to_map, giant_scc, owned_range, pivot, reach, scc, split_rows, trim1
 
 
 class CpuOps:
@@ -85,11 +88,27 @@ def _worker(rank, world, port, q, kind="planted"):
         dist.destroy_process_group()
 
 
-def _run_world(world, kind):
+def _worker_scc(rank, world, port, q, kind="planted"):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=30))
+    try:
+        g = _graph() if kind == "planted" else _graph_rmat()
+        exact = oracle.tarjan(g)
+        fw = split_rows(g.fw_beg, g.fw_adj, rank, world)
+        bw = split_rows(g.bw_beg, g.bw_adj, rank, world)
+        labels = scc(fw, bw, g.V, solve=oracle.tarjan, ops=CpuOps, device="cpu")
+        q.put((rank, bool(np.array_equal(labels, exact))))
+    except Exception as e:  # noqa: BLE001
+        q.put((rank, repr(e)))
+    finally:
+        dist.destroy_process_group()
+
+
+def _run_world(world, kind, target=None):
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _port()
-    ps = [ctx.Process(target=_worker, args=(r, world, port, q, kind)) for r in range(world)]
+    ps = [ctx.Process(target=target or _worker, args=(r, world, port, q, kind)) for r in range(world)]
     for p in ps:
         p.start()
     for p in ps:
@@ -173,3 +192,36 @@ def test_seed_set_and_empty_graph():
     e = split_rows(np.zeros(41, np.int64), np.zeros(0, np.int32), 0, 1)
     assert int(bits_to_map(reach(e, 40, [7], None, ops=CpuOps, device="cpu"), 40).sum()) == 1
     del exact
+
+
+def test_sharded_detection_world_size_2():
+    """The whole detection over sharded rows: every rank ends with the exact
+    labels (trim-1, the giant by the sharded searches, the residual gathered
+    and solved; the oracle stands in for the single-GPU engine)."""
+    res = _run_world(2, "planted", _worker_scc)
+    assert res == [(0, True), (1, True)], res
+
+
+def test_sharded_detection_world_size_3_uneven_rows():
+    res = _run_world(3, "rmat", _worker_scc)
+    assert res == [(0, True), (1, True), (2, True)], res
+
+
+def test_sharded_detection_one_rank_and_trim():
+    """One process: labels exact; trim-1 removes exactly vertices that are
+    their own SCC; the pivot is active and has the largest degree product."""
+    for g in (_graph(), _graph_rmat(), G.toy()):
+        exact = oracle.tarjan(g)
+        fw = split_rows(g.fw_beg, g.fw_adj, 0, 1)
+        bw = split_rows(g.bw_beg, g.bw_adj, 0, 1)
+        assert np.array_equal(scc(fw, bw, g.V, solve=oracle.tarjan, ops=CpuOps, device="cpu"), exact)
+        active, trimmed = trim1(fw, bw, g.V, rounds=10, device="cpu")
+        act = bits_to_map(active, g.V).numpy().astype(bool)
+        tr = bits_to_map(trimmed, g.V).numpy().astype(bool)
+        assert not (act & tr).any() and (act | tr).all()
+        sizes = np.bincount(exact, minlength=g.V)
+        assert (sizes[exact[tr]] == 1).all()  # trimmed vertices are singleton SCCs
+        p = pivot(fw, bw, g.V, active)
+        if act.any():
+            prod = np.diff(g.fw_beg).astype(np.int64) * np.diff(g.bw_beg)
+            assert act[p] and prod[p] == prod[act].max() and p == np.nonzero(act & (prod == prod[p]))[0][0]
