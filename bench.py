@@ -56,7 +56,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 REF_PARAMS = ("30", "200", "10", "0.1")  # src/bash_one.sh:4
-KERNELS_PER_STEP = 18  # stage kernels enqueued per pipeline run (pipeline.cu: enqueue)
+KERNELS_PER_STEP = 27  # stage kernels enqueued per pipeline run (pipeline.cu: enqueue; the launch list of the social run)
 
 
 def log(*a):
